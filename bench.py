@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Benchmark: MPS two-site updates/s at chi_max = 64 on B200.
+
+Workload (one "step"): a 100-qubit open chain in |0...0>, depth-20 brick-wall
+of Haar-random 4x4 gates (seeded), chi_max = 64, cutoff 1e-10 -- 990 two-site
+updates, each layer's 49-50 disjoint pairs in one launch.  Synthetic gates;
+no dataset is involved.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+``value`` is device-timed (CUDA events, inputs resident in HBM, L2 flushed
+between steps) updates/s over all ranks; ``e2e`` runs the same circuit
+through the public Python API (``MPSState.apply_layer``) with the gates copied
+from pinned host memory and the final MPS read back every step.  With
+--gpus N > 1 (launched by torch.distributed.run) every rank advances its own
+replica circuit (different seed): no collective on the data path, timing is
+the max over ranks.  ``--impl reference`` times the CPU restatement of the
+reference engine (scipy gesdd) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "MPS 2-site updates/s at chi=64 and grad s/step: mixed vs FP64 GPU, err≤1e-6"
+UNIT = "updates/s"
+N_SITES, DEPTH, CHI, CUTOFF, SEED = 100, 20, 64, 1e-10, 2024
+WORKLOAD = (f"MPS two-site updates: n={N_SITES} open chain, depth-{DEPTH} Haar brick-wall, "
+            f"chi_max={CHI}, cutoff={CUTOFF:g}, each layer's pairs in one launch")
+
+
+# ----------------------------------------------------------------- counting
+def update_flops(cl: int, cm: int, cr: int) -> float:
+    """Algorithmic flops of one update: contraction 32 cl cm cr, gate 128 cl cr,
+    nominal complex SVD 4 (14 m n^2 + 8 n^3) with m >= n the sides of theta."""
+    m, n = 2 * cl, 2 * cr
+    if m < n:
+        m, n = n, m
+    return 32.0 * cl * cm * cr + 128.0 * cl * cr + 4.0 * (14.0 * m * n * n + 8.0 * n ** 3)
+
+
+def update_bytes(cl: int, cm: int, cr: int, k: int) -> float:
+    """Site-tensor HBM bytes of one update: read A, B and the gate, write A', B'."""
+    return 16.0 * (2 * cl * cm + 2 * cm * cr + 2 * cl * k + 2 * k * cr) + 256.0
+
+
+def replay_dims(n: int, layer_sites, layer_kept):
+    """Pre-update (chi_l, chi_m, chi_r, kept) of every pair, replayed from the kept counts."""
+    bonds = [1] * (n + 1)
+    out = []
+    for sites, kept in zip(layer_sites, layer_kept):
+        per = []
+        for i, k in zip(sites, kept):
+            per.append((bonds[i], bonds[i + 1], bonds[i + 2], int(k)))
+        for i, k in zip(sites, kept):
+            bonds[i + 1] = int(k)
+        out.append(per)
+    return out
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples taken while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", gpu_id, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- CPU side
+def cpu_baseline_sample(workers: int):
+    from oracle.cpu_baseline import make_pool, run_parallel
+    pool = make_pool(workers)
+    try:
+        run_parallel(8, 2, 4, CUTOFF, workers, seed=SEED, pool=pool)  # spawn + import outside the timing
+        r = run_parallel(N_SITES, DEPTH, CHI, CUTOFF, workers, reps=1, seed=SEED, pool=pool)
+    finally:
+        pool.close()
+        pool.join()
+    return {"value": round(r["updates_per_s"], 3), "unit": UNIT, "cores": workers, "kind": "port",
+            "sample": (f"{workers} single-BLAS-thread processes, each one full n={N_SITES} depth-{DEPTH} "
+                       f"chi={CHI} circuit ({r['updates']} updates, {r['wall_s']:.1f} s wall); oracle "
+                       "restatement of mps_core.py with scipy gesdd")}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.cpu_baseline import make_pool, run_parallel, usable_cores
+    workers = usable_cores()
+    pool = make_pool(workers)
+    try:
+        for _ in range(args.warmup):
+            run_parallel(N_SITES, DEPTH, CHI, CUTOFF, workers, seed=SEED, pool=pool)
+        t0 = time.perf_counter()
+        total = 0
+        for _ in range(args.steps):
+            total += run_parallel(N_SITES, DEPTH, CHI, CUTOFF, workers, seed=SEED, pool=pool)["updates"]
+        dt = time.perf_counter() - t0
+    finally:
+        pool.close()
+        pool.join()
+    value = total / dt
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * dt / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Haar gates)",
+            "config": {"workload": WORKLOAD, "parallelism": f"{workers} host processes x 1 circuit each"},
+            "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": workers, "kind": "port",
+                             "sample": f"{workers} processes x one full circuit per step"},
+            "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- GPU side
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+    from fpga_mps_simulator_b200 import MPSBatch, MPSState, _lib
+    from fpga_mps_simulator_b200.circuits import brickwall_layers
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    lib = _lib.load()
+    precision = args.precision
+
+    # ---- CPU baseline first (spawned workers, before heavy GPU work; rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle.cpu_baseline import usable_cores
+        cpu = cpu_baseline_sample(usable_cores())
+
+    layers = brickwall_layers(N_SITES, DEPTH, SEED + rank)
+    n_upd = sum(len(L.sites) for L in layers)
+    batch = MPSBatch([N_SITES], [CHI], [CUTOFF], precision=precision, device=dev)
+    pbs = [batch.make_pairs(np.zeros(len(L.sites), np.int32), L.sites, L.gates) for L in layers]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def reset(b):
+        b.sites.zero_()
+        b.sites[:, 0] = 1.0
+        b.bonds.fill_(1)
+        b.norm_logs.zero_()
+        b.status_acc.zero_()
+
+    def step():
+        reset(batch)
+        for pb in pbs:
+            batch.run_pairs(pb)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- FP64 peak probe (the roofline denominator for the FP64-bound kernel)
+    props = torch.cuda.get_device_properties(dev)
+    sink = torch.zeros(1, dtype=torch.float64, device=dev)
+    probe_blocks, probe_threads, probe_iters = props.multi_processor_count * 8, 256, 1 << 16
+    s = torch.cuda.current_stream(dev)
+    for _ in range(2):
+        _lib.check(lib.mpsb_fp64_probe(probe_iters, probe_blocks, probe_threads, sink.data_ptr(), s.cuda_stream),
+                   "fp64 probe")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    _lib.check(lib.mpsb_fp64_probe(probe_iters, probe_blocks, probe_threads, sink.data_ptr(), s.cuda_stream),
+               "fp64 probe")
+    e1.record()
+    torch.cuda.synchronize()
+    fp64_peak_tflops = probe_blocks * probe_threads * probe_iters * 16.0 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+    # ---- warm-up
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    batch.check_status()
+
+    # ---- timed region: K steps, per-step and per-layer CUDA events, L2 flushed between steps
+    gpu_id = "GPU-" + str(props.uuid) if hasattr(props, "uuid") else str(local)
+    clocks = ClockSampler(gpu_id)
+    barrier()
+    torch.cuda.synchronize()
+    step_ms, layer_ms = [], np.zeros(len(layers))
+    for _ in range(args.steps):
+        flush.zero_()
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(layers) + 2)]
+        evs[0].record()
+        reset(batch)
+        evs[1].record()
+        for li, pb in enumerate(pbs):
+            batch.run_pairs(pb)
+            evs[li + 2].record()
+        torch.cuda.synchronize()
+        step_ms.append(evs[0].elapsed_time(evs[-1]))
+        for li in range(len(layers)):
+            layer_ms[li] += evs[li + 1].elapsed_time(evs[li + 2])
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    batch.check_status()
+    total_s = max_over_ranks(sum(step_ms) * 1e-3)
+    value = world * n_upd * args.steps / total_s
+
+    # ---- roofline of the update kernel (algorithmic flops / launch time)
+    kept = [pb.kept.cpu().numpy() for pb in pbs]
+    dims = replay_dims(N_SITES, [L.sites for L in layers], kept)
+    flops = sum(update_flops(cl, cm, cr) for per in dims for cl, cm, cr, _ in per)
+    hbm = sum(update_bytes(cl, cm, cr, k) for per in dims for cl, cm, cr, k in per)
+    kern_s = layer_ms.sum() * 1e-3 / args.steps
+    achieved_tf = flops / kern_s / 1e12
+    sat = [li for li, per in enumerate(dims) if all(d[0] == CHI and d[1] == CHI and d[2] == CHI for d in per[1:-1])]
+    sat_rate = (sum(len(dims[li]) for li in sat) / (layer_ms[sat].sum() * 1e-3 / args.steps)) if sat else None
+
+    # ---- per-update drop-in path (one update per call, no batching), one layer
+    single = None
+    if not args.quick:
+        st1 = MPSState(N_SITES, CHI, CUTOFF, precision=precision, device=dev)
+        st1._b.sites.copy_(batch.sites)
+        st1._b.bonds.copy_(batch.bonds)
+        L = layers[-1]
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for i, g in zip(L.sites, L.gates):
+            st1._apply_adjacent_2q(int(i), g)
+        a1.record()
+        torch.cuda.synchronize()
+        single = {"updates_per_s": round(len(L.sites) / (a0.elapsed_time(a1) * 1e-3), 3),
+                  "note": "MPSState._apply_adjacent_2q one pair per launch, saturated chi=64 layer"}
+
+    # ---- end to end through the public API, gates from pinned host memory, MPS read back
+    e2e = None
+    if not args.quick:
+        st = MPSState(N_SITES, CHI, CUTOFF, precision=precision, device=dev)
+        pinned = [torch.from_numpy(np.ascontiguousarray(L.gates)).pin_memory() for L in layers]
+        ones = torch.ones(N_SITES, dtype=torch.complex128).pin_memory()
+        out_sites = torch.empty(st._b.sites.shape, dtype=torch.complex128).pin_memory()
+        out_bonds = torch.empty(N_SITES + 1, dtype=torch.int32).pin_memory()
+        out_nl = torch.empty(1, dtype=torch.float64).pin_memory()
+        h2d = sum(p.numel() * 16 for p in pinned) + sum(len(L.sites) * 16 for L in layers) + N_SITES * 16
+        d2h = out_sites.numel() * 16 + out_bonds.numel() * 4 + 8
+
+        def e2e_step():
+            b = st._b
+            b.sites.zero_()
+            b.sites[:, 0].copy_(ones, non_blocking=True)
+            b.bonds.fill_(1)
+            b.norm_logs.zero_()
+            for L, g in zip(layers, pinned):
+                st.apply_layer(L.sites, g)
+            out_sites.copy_(b.sites, non_blocking=True)
+            out_bonds.copy_(b.bonds, non_blocking=True)
+            out_nl.copy_(b.norm_logs, non_blocking=True)
+            torch.cuda.current_stream(dev).synchronize()
+
+        e2e_step()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        st.check_status()
+        e2e = {"value": round(world * n_upd * args.steps / e2e_s, 3), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_s * 1e3 / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f64+tf32x3",
+        "data": "synthetic (seeded Haar-random 4x4 gates, |0...0> start)",
+        "config": {"workload": WORKLOAD, "precision": precision, "updates_per_step": n_upd,
+                   "launches_per_step": 2 * len(layers), "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "flushed between steps (256 MiB write)"},
+        "roofline": {"bound": "fp64", "achieved": round(achieved_tf, 4), "peak": round(fp64_peak_tflops, 4),
+                     "unit": "TFLOP/s", "frac": round(achieved_tf / fp64_peak_tflops, 4), "traffic": None,
+                     "peak_source": "measured: FP64 FMA probe (mpsb_fp64_probe) on this GPU, burst",
+                     "kernel": "update2q_fp64_kernel (+fold_norm_log_kernel)",
+                     "flops_per_step": flops, "hbm_site_bytes_per_step": hbm,
+                     "hbm_gbs": round(hbm / kern_s / 1e9, 3),
+                     "saturated_layer_updates_per_s": None if sat_rate is None else round(sat_rate, 3)},
+        "gpu_launches": 2 * len(layers) * args.steps,
+        "clocks": clk,
+        "e2e": e2e,
+        "per_update_path": single,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--quick", action="store_true", help="skip the e2e and per-update legs")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,104 @@
+"""ctypes binding of libmpsb200.so (the C ABI declared in include/mpsb200.h).
+
+The library is loaded from the package directory.  There is no fallback: if
+the shared object is missing or no sm_100 device is present, every entry point
+raises, so the GPU path can never silently become a CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmpsb200.so")
+
+MPSB_CHI_LIMIT = 64
+FP64 = 0
+MIXED_TF32X3 = 1
+ST_NOCONV, ST_NONFINITE, ST_BADDIM = 1, 2, 4
+_ERRORS = {-1: "EINVAL", -2: "ELAUNCH", -3: "EWORKSPACE", -4: "ENODEV"}
+
+# Symbols the header declares; tests check that every one is exported.
+EXPORTS = (
+    "mpsb_version", "mpsb_last_error", "mpsb_update2q_workspace_bytes", "mpsb_update2q_batch",
+    "mpsb_apply1q_batch", "mpsb_statevector", "mpsb_amplitude", "mpsb_expect_workspace_bytes",
+    "mpsb_expect_local", "mpsb_fp64_probe",
+)
+
+
+class Chain(C.Structure):
+    """mpsb_chain."""
+    _fields_ = [
+        ("sites", C.c_void_p),
+        ("bonds", C.c_void_p),
+        ("norm_log", C.c_void_p),
+        ("status_acc", C.c_void_p),
+        ("slot_elems", C.c_int64),
+        ("n", C.c_int32),
+        ("chi_max", C.c_int32),
+        ("cutoff", C.c_double),
+    ]
+
+
+class Pair(C.Structure):
+    """mpsb_pair."""
+    _fields_ = [("chain", C.c_int32), ("site", C.c_int32), ("gate", C.c_int32), ("out", C.c_int32)]
+
+
+class SiteOp(C.Structure):
+    """mpsb_site_op."""
+    _fields_ = [("chain", C.c_int32), ("site", C.c_int32), ("gate", C.c_int32), ("pad", C.c_int32)]
+
+
+class MPSBError(RuntimeError):
+    """A C-ABI call returned an error code."""
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def _declare(lib):
+    vp, i32, i64, sz, dbl = C.c_void_p, C.c_int, C.c_int64, C.c_size_t, C.c_double
+    sig = {
+        "mpsb_version": (C.c_char_p, []),
+        "mpsb_last_error": (C.c_char_p, []),
+        "mpsb_update2q_workspace_bytes": (sz, [i32, i32]),
+        "mpsb_update2q_batch": (i32, [vp, vp, i32, vp, i32, i32, dbl, i32, vp, sz, vp, vp, vp, vp, vp]),
+        "mpsb_apply1q_batch": (i32, [vp, vp, i32, vp, i32, vp]),
+        "mpsb_statevector": (i32, [vp, i32, i32, vp, vp, sz, vp]),
+        "mpsb_amplitude": (i32, [vp, i32, i32, vp, i32, i32, vp, vp, vp]),
+        "mpsb_expect_workspace_bytes": (sz, [i32, i32, i32]),
+        "mpsb_expect_local": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp, vp, sz, vp]),
+        "mpsb_fp64_probe": (i32, [i64, i32, i32, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def load(path: str = LIB_PATH):
+    """Load (once) and return the library handle."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(path):
+                raise ImportError(
+                    f"{path} is missing: build it with `python -m fpga_mps_simulator_b200.build` "
+                    "(there is no CPU fallback)")
+            lib = C.CDLL(path)
+            _declare(lib)
+            _lib = lib
+    return _lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = load().mpsb_last_error().decode(errors="replace")
+        raise MPSBError(f"{what} failed ({_ERRORS.get(rc, rc)}): {msg}")
+
+
+def version() -> str:
+    return load().mpsb_version().decode()

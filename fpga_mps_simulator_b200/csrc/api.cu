@@ -1,0 +1,173 @@
+// C ABI of libmpsb200 (declared in include/mpsb200.h): argument checks,
+// error reporting and dispatch to the kernels.
+#include "mpsb_common.cuh"
+
+#include <cstdarg>
+#include <cstdio>
+
+namespace mpsb {
+
+static thread_local char g_err[512] = "";
+
+int set_error(int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int check_launch(const char *what) {
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(MPSB_ELAUNCH, "%s: %s", what, cudaGetErrorString(e));
+    return MPSB_OK;
+}
+
+static int check_device() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_error(MPSB_ENODEV, "no CUDA device");
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    if (major != 10) return set_error(MPSB_ENODEV, "device %d has compute capability %d.x; sm_100 required", dev, major);
+    return MPSB_OK;
+}
+
+// kernels (update2q.cu, readout.cu)
+size_t upd_workspace_bytes(int npairs, int chi_cap);
+int launch_update2q(const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int, void *,
+                    double *, int32_t *, double *, int32_t *, cudaStream_t);
+int launch_update2q_mixed(const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int, void *,
+                          double *, int32_t *, double *, int32_t *, cudaStream_t);
+int launch_apply1q(const mpsb_chain *, const mpsb_site_op *, int, const double2 *, int, cudaStream_t);
+int launch_statevector(const mpsb_chain *, int, int, double2 *, double2 *, size_t, cudaStream_t);
+int launch_amplitude(const mpsb_chain *, int, int, const uint8_t *, int, double2 *, double *, cudaStream_t);
+size_t expect_workspace_bytes(int nchains, int n, int chi_cap, int nctas);
+int launch_expect(const mpsb_chain *, int, int, int, const int32_t *, const int32_t *, const double2 *, int,
+                  double *, void *, int, cudaStream_t);
+int launch_fp64_probe(long long iters, int blocks, int threads, double *sink, cudaStream_t s);
+
+static int expect_ctas() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return 2 * sms;
+}
+
+}  // namespace mpsb
+
+using namespace mpsb;
+
+extern "C" {
+
+const char *mpsb_version(void) { return "libmpsb200 1.0 (sm_100a)"; }
+
+const char *mpsb_last_error(void) { return g_err; }
+
+size_t mpsb_update2q_workspace_bytes(int npairs, int chi_cap) {
+    if (npairs < 0 || chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT) return 0;
+    return upd_workspace_bytes(npairs, chi_cap);
+}
+
+int mpsb_update2q_batch(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const mpsb_c128 *gates,
+                        int precision, int chi_cap, double tol, int max_sweeps, void *workspace,
+                        size_t workspace_bytes, double *spectra, int32_t *kept, double *trunc, int32_t *status,
+                        mpsb_stream_t stream) {
+    if (npairs < 0) return set_error(MPSB_EINVAL, "npairs=%d < 0", npairs);
+    if (npairs == 0) return MPSB_OK;
+    if (!chains || !pairs || !gates || !status || !workspace)
+        return set_error(MPSB_EINVAL, "null chains/pairs/gates/status/workspace pointer");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3)
+        return set_error(MPSB_EINVAL, "unknown precision %d", precision);
+    const size_t need = upd_workspace_bytes(npairs, chi_cap);
+    if (workspace_bytes < need)
+        return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+        return set_error(MPSB_EINVAL, "workspace must be 256-byte aligned");
+    int rc = check_device();
+    if (rc) return rc;
+    if (max_sweeps <= 0) max_sweeps = 40;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const double2 *g = reinterpret_cast<const double2 *>(gates);
+    if (precision == MPSB_FP64) {
+        if (tol <= 0.0) tol = 1.0e-14;
+        return launch_update2q(chains, pairs, npairs, g, chi_cap, tol, max_sweeps, workspace, spectra, kept, trunc,
+                               status, s);
+    }
+    if (tol <= 0.0) tol = 1.0e-9;
+    return launch_update2q_mixed(chains, pairs, npairs, g, chi_cap, tol, max_sweeps, workspace, spectra, kept,
+                                 trunc, status, s);
+}
+
+int mpsb_apply1q_batch(const mpsb_chain *chains, const mpsb_site_op *ops, int nops, const mpsb_c128 *gates,
+                       int chi_cap, mpsb_stream_t stream) {
+    if (nops < 0) return set_error(MPSB_EINVAL, "nops=%d < 0", nops);
+    if (nops == 0) return MPSB_OK;
+    if (!chains || !ops || !gates) return set_error(MPSB_EINVAL, "null chains/ops/gates pointer");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_apply1q(chains, ops, nops, reinterpret_cast<const double2 *>(gates), chi_cap,
+                          reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mpsb_statevector(const mpsb_chain *chain_dev, int n, int chi_cap, mpsb_c128 *out, mpsb_c128 *scratch,
+                     size_t scratch_bytes, mpsb_stream_t stream) {
+    if (!chain_dev || !out || !scratch) return set_error(MPSB_EINVAL, "null chain/out/scratch pointer");
+    if (n < 1 || n > 24) return set_error(MPSB_EINVAL, "statevector needs 1 <= n <= 24, got %d", n);
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_statevector(chain_dev, n, chi_cap, reinterpret_cast<double2 *>(out),
+                              reinterpret_cast<double2 *>(scratch), scratch_bytes,
+                              reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mpsb_amplitude(const mpsb_chain *chains, int chain, int n, const uint8_t *bits, int nbits, int chi_cap,
+                   mpsb_c128 *out, double *log_abs, mpsb_stream_t stream) {
+    if (!chains || !bits || !out) return set_error(MPSB_EINVAL, "null chains/bits/out pointer");
+    if (nbits < 0 || n < 1 || chain < 0) return set_error(MPSB_EINVAL, "bad nbits/n/chain");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_amplitude(chains, chain, n, bits, nbits, reinterpret_cast<double2 *>(out), log_abs,
+                            reinterpret_cast<cudaStream_t>(stream));
+}
+
+size_t mpsb_expect_workspace_bytes(int nchains, int n, int chi_cap) {
+    if (nchains < 0 || n < 1 || chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT) return 0;
+    return expect_workspace_bytes(nchains, n, chi_cap, expect_ctas());
+}
+
+int mpsb_expect_local(const mpsb_chain *chains, int nchains, int n, int chi_cap, const int32_t *sites,
+                      const int32_t *two_site, const mpsb_c128 *ops, int nterms, double *out, void *workspace,
+                      size_t workspace_bytes, mpsb_stream_t stream) {
+    if (nchains < 0 || nterms < 0 || n < 1) return set_error(MPSB_EINVAL, "bad nchains/nterms/n");
+    if (nchains == 0 || nterms == 0) return MPSB_OK;
+    if (!chains || !sites || !two_site || !ops || !out || !workspace)
+        return set_error(MPSB_EINVAL, "null pointer argument");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    const int nctas = expect_ctas();
+    const size_t need = expect_workspace_bytes(nchains, n, chi_cap, nctas);
+    if (workspace_bytes < need)
+        return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_expect(chains, nchains, n, chi_cap, sites, two_site, reinterpret_cast<const double2 *>(ops),
+                         nterms, out, workspace, nctas, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mpsb_fp64_probe(int64_t iters, int blocks, int threads, double *sink, mpsb_stream_t stream) {
+    if (iters < 1 || blocks < 1 || threads < 32 || threads > 1024 || !sink)
+        return set_error(MPSB_EINVAL, "bad probe arguments");
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_fp64_probe(iters, blocks, threads, sink, reinterpret_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

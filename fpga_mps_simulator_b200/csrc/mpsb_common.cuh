@@ -1,0 +1,73 @@
+// Shared device helpers for libmpsb200: complex128 arithmetic on double2,
+// warp reductions, error plumbing.  sm_100a only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cooperative_groups.h>
+#include <stdint.h>
+
+#include "mpsb200.h"
+
+namespace mpsb {
+namespace cg = cooperative_groups;
+
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ < 1000)
+#error "libmpsb200 is built for sm_100a only"
+#endif
+
+// ---------------------------------------------------------------- complex
+__device__ __forceinline__ double2 c_make(double re, double im) { return make_double2(re, im); }
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 c_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 c_conj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 c_scale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 c_mul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// acc + a * b
+__device__ __forceinline__ double2 c_fma(double2 a, double2 b, double2 acc) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+    return acc;
+}
+// acc + conj(a) * b
+__device__ __forceinline__ double2 c_cfma(double2 a, double2 b, double2 acc) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(-a.y, b.x, acc.y);
+    return acc;
+}
+__device__ __forceinline__ double c_abs2(double2 a) { return fma(a.x, a.x, a.y * a.y); }
+__device__ __forceinline__ bool c_finite(double2 a) { return isfinite(a.x) && isfinite(a.y); }
+
+__device__ __forceinline__ double2 ld_c(const mpsb_c128 *p) {
+    return __ldg(reinterpret_cast<const double2 *>(p));
+}
+
+// ---------------------------------------------------------------- warp
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Per-pair bookkeeping written by the update kernel, folded into norm_log by
+// a second kernel in pair order.
+struct PairRec {
+    double d_trunc;   // 0.5*log(1 - dropped/total) (0 when nothing dropped)
+    double d_norm;    // log(norm of kept S) (0 when norm <= 1e-15)
+    double discarded; // dropped/total
+    int32_t keep;
+    int32_t status;
+};
+
+}  // namespace mpsb
+
+// host-side error helpers (defined in api.cu)
+namespace mpsb {
+int set_error(int code, const char *fmt, ...);
+int check_launch(const char *what);
+}  // namespace mpsb

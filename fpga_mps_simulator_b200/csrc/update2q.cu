@@ -1,0 +1,596 @@
+// Fused MPS two-site update for sm_100a: contract -> gate -> one-sided Jacobi
+// truncated SVD -> renormalise -> sqrt(S) split, one thread-block cluster of
+// two CTAs per pair.
+//
+// Semantics follow mps_core.py:326-350 (_apply_adjacent_2q) and
+// mps_core.py:277-300 (_svd_truncate) of nasir26/fpga-mps-simulator; the
+// contraction is the one fpga_mps_simulator.cpp:287-371 offloads.
+//
+// Design (one pair):
+//   M = theta as (2 chi_l) x (2 chi_r).  The Jacobi works on X = M when
+//   chi_r <= chi_l, else on X = M^H, so X has R >= C rows and C <= 128
+//   columns.  Columns are split between the two CTAs (C_pad/2 each, C_pad =
+//   C rounded up to 8, zero-padded) and live in shared memory as FP64
+//   complex, column-major (up to 128 KB per CTA at chi = 64).  Each CTA
+//   holds two "slots" (blocks) of w = C_pad/4 columns.  A sweep covers all
+//   C_pad (C_pad-1)/2 column pairs: the pairs inside each block plus the six
+//   block pairs, three steps with the blocks exchanged between the CTAs
+//   through distributed shared memory after each step.  Inside a CTA a warp
+//   owns a "duo pair" (two columns of each of two blocks) per round and
+//   performs four rotations with the columns in registers, so shared memory
+//   moves two columns per rotation.  The right singular vectors are not
+//   accumulated: the small side of the split is recovered at the end as
+//   Y = X_k^H X0 from the unrotated theta X0 (kept in the workspace), which
+//   keeps the product U S Vh exact to rounding (checked against the reference
+//   over full circuits).
+#include "mpsb_common.cuh"
+
+#include <cstdio>
+
+namespace mpsb {
+
+constexpr int kUpdThreads = 512;
+constexpr int kUpdWarps = kUpdThreads / 32;
+
+struct Upd2Params {
+    const mpsb_chain *chains;
+    const mpsb_pair *pairs;
+    int npairs;
+    const double2 *gates;
+    double2 *x0;          // workspace: unrotated X per pair
+    long long x0_stride;  // complex elements per pair
+    PairRec *rec;         // workspace: per-pair records
+    double *spectra;
+    int32_t *kept;
+    double *trunc;
+    int32_t *status;
+    int chi_cap;
+    int wmax;             // column capacity of a slot
+    int rpad;             // row capacity of a column (multiple of 32)
+    double tol2;          // squared Jacobi tolerance
+    int max_sweeps;
+};
+
+struct CtaScalars {
+    int nrot[2];
+    int nonfinite;
+    int keep;
+    int nk;
+    int pad0;
+    double div;
+    double2 gate[16];
+};
+
+__host__ __device__ inline size_t upd_smem_bytes(int wmax, int rpad) {
+    return 384 + (size_t)3 * wmax * rpad * sizeof(double2) + (size_t)2 * wmax * sizeof(double) +
+           (size_t)4 * wmax * sizeof(double) + (size_t)4 * wmax * sizeof(int);
+}
+
+// ------------------------------------------------------------- rotations
+// One complex Jacobi rotation of columns (x, y) given the reduced Gram
+// entries a = |x|^2, b = |y|^2, g = x^H y.  With g = |g| e^{i phi} the pair is
+// the real problem [[a,|g|],[|g|,b]] in the basis (x, e^{-i phi} y); the
+// classical Jacobi angle zeta = (b-a)/(2|g|), t = sgn(zeta)/(|zeta| +
+// sqrt(1+zeta^2)), c = 1/sqrt(1+t^2), s = c t gives
+//   x' = c x - s e^{-i phi} y,  y' = s x + c e^{-i phi} y.
+template <int RPL>
+__device__ __forceinline__ int apply_rotation(double2 (&x)[RPL], double2 (&y)[RPL], double a, double b,
+                                              double gr, double gi, double tol2) {
+    const double g2 = fma(gr, gr, gi * gi);
+    if (!(g2 > tol2 * (a * b))) return 0;  // converged pair (also rejects NaN)
+    const double rg = rsqrt(g2);
+    const double zeta = 0.5 * (b - a) * rg;
+    double t = 1.0 / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
+    t = copysign(t, zeta);
+    const double c = rsqrt(fma(t, t, 1.0));
+    const double s = c * t;
+    const double er = gr * rg, ei = gi * rg;
+    const double2 zp = make_double2(-s * er, s * ei);  // -s conj(e)
+    const double2 zq = make_double2(c * er, -c * ei);  //  c conj(e)
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+        const double2 xo = x[r], yo = y[r];
+        x[r] = c_fma(zp, yo, c_scale(xo, c));
+        y[r] = c_fma(zq, yo, c_scale(xo, s));
+    }
+    return 1;
+}
+
+template <int RPL>
+__device__ __forceinline__ void gram_partial(const double2 (&x)[RPL], const double2 (&y)[RPL], double &a,
+                                             double &b, double &gr, double &gi) {
+    a = 0.0; b = 0.0; gr = 0.0; gi = 0.0;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+        a = fma(x[r].x, x[r].x, fma(x[r].y, x[r].y, a));
+        b = fma(y[r].x, y[r].x, fma(y[r].y, y[r].y, b));
+        gr = fma(x[r].x, y[r].x, fma(x[r].y, y[r].y, gr));
+        gi = fma(x[r].x, y[r].y, fma(-x[r].y, y[r].x, gi));
+    }
+}
+
+// Two independent rotations, reductions interleaved for ILP.
+template <int RPL>
+__device__ __forceinline__ int rotate2(double2 (&x1)[RPL], double2 (&y1)[RPL], double2 (&x2)[RPL],
+                                       double2 (&y2)[RPL], double tol2) {
+    double v[8];
+    gram_partial<RPL>(x1, y1, v[0], v[1], v[2], v[3]);
+    gram_partial<RPL>(x2, y2, v[4], v[5], v[6], v[7]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+    int n = apply_rotation<RPL>(x1, y1, v[0], v[1], v[2], v[3], tol2);
+    n += apply_rotation<RPL>(x2, y2, v[4], v[5], v[6], v[7], tol2);
+    return n;
+}
+
+template <int RPL>
+__device__ __forceinline__ int rotate1(double2 (&x)[RPL], double2 (&y)[RPL], double tol2) {
+    double v[4];
+    gram_partial<RPL>(x, y, v[0], v[1], v[2], v[3]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    }
+    return apply_rotation<RPL>(x, y, v[0], v[1], v[2], v[3], tol2);
+}
+
+template <int RPL>
+__device__ __forceinline__ void load_col(const double2 *col, int lane, double2 (&v)[RPL]) {
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) v[r] = col[lane + 32 * r];
+}
+template <int RPL>
+__device__ __forceinline__ void store_col(double2 *col, int lane, const double2 (&v)[RPL]) {
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) col[lane + 32 * r] = v[r];
+}
+
+// Warp task: the four cross rotations between duo (p0,p1) and duo (q0,q1).
+template <int RPL>
+__device__ __forceinline__ int duo_pair(double2 *p0c, double2 *p1c, double2 *q0c, double2 *q1c, int lane,
+                                        double tol2) {
+    double2 p0[RPL], p1[RPL], q0[RPL], q1[RPL];
+    load_col<RPL>(p0c, lane, p0);
+    load_col<RPL>(p1c, lane, p1);
+    load_col<RPL>(q0c, lane, q0);
+    load_col<RPL>(q1c, lane, q1);
+    int n = rotate2<RPL>(p0, q0, p1, q1, tol2);
+    n += rotate2<RPL>(p0, q1, p1, q0, tol2);
+    store_col<RPL>(p0c, lane, p0);
+    store_col<RPL>(p1c, lane, p1);
+    store_col<RPL>(q0c, lane, q0);
+    store_col<RPL>(q1c, lane, q1);
+    return n;
+}
+
+template <int RPL>
+__device__ __forceinline__ int duo_single(double2 *c0, double2 *c1, int lane, double tol2) {
+    double2 x[RPL], y[RPL];
+    load_col<RPL>(c0, lane, x);
+    load_col<RPL>(c1, lane, y);
+    const int n = rotate1<RPL>(x, y, tol2);
+    store_col<RPL>(c0, lane, x);
+    store_col<RPL>(c1, lane, y);
+    return n;
+}
+
+// Element at position k of round r of the circle-method round robin over nd2 items.
+__device__ __forceinline__ int rr_elem(int k, int r, int nd2) {
+    return k == 0 ? 0 : 1 + (k - 1 + r) % (nd2 - 1);
+}
+
+// One block-step of a sweep inside a CTA: (optionally) all pairs inside each
+// of the two slots, then all pairs between slot 0 and slot 1.
+template <int RPL>
+__device__ void step_rounds(double2 *X, int w, int wmax, int rpad, bool internal, int warp, int lane,
+                            double tol2, int &cnt) {
+    const int nd = w >> 1;
+    auto col = [&](int slot, int j) { return X + (size_t)(slot * wmax + j) * rpad; };
+    if (internal) {
+        for (int t = warp; t < 2 * nd; t += kUpdWarps) {
+            const int slot = t / nd, d = t - slot * nd;
+            cnt += duo_single<RPL>(col(slot, 2 * d), col(slot, 2 * d + 1), lane, tol2);
+        }
+        __syncthreads();
+        const int nd2 = nd + (nd & 1);
+        const int half = nd2 >> 1;
+        for (int r = 0; r < nd2 - 1; ++r) {
+            for (int t = warp; t < 2 * half; t += kUpdWarps) {
+                const int slot = t / half, k = t - slot * half;
+                const int u = rr_elem(k, r, nd2), v = rr_elem(nd2 - 1 - k, r, nd2);
+                if (u < nd && v < nd)
+                    cnt += duo_pair<RPL>(col(slot, 2 * u), col(slot, 2 * u + 1), col(slot, 2 * v),
+                                         col(slot, 2 * v + 1), lane, tol2);
+            }
+            __syncthreads();
+        }
+    }
+    for (int r = 0; r < nd; ++r) {
+        for (int t = warp; t < nd; t += kUpdWarps) {
+            int v = t + r;
+            if (v >= nd) v -= nd;
+            cnt += duo_pair<RPL>(col(0, 2 * t), col(0, 2 * t + 1), col(1, 2 * v), col(1, 2 * v + 1), lane,
+                                 tol2);
+        }
+        __syncthreads();
+    }
+}
+
+// Swap one slot with the partner CTA.  Pattern A (parity 0): CTA0.slot1 <->
+// CTA1.slot0; pattern B (parity 1): CTA0.slot1 <-> CTA1.slot1.  Alternating
+// A, B, A, ... after every step visits all six block pairs once per sweep.
+// Each CTA stores its outgoing block into the partner's staging area through
+// distributed shared memory, then copies its own staging area into the slot.
+__device__ void exchange_slots(cg::cluster_group &cluster, double2 *X, double2 *stage, int crank, int parity,
+                               int w, int wmax, int rpad, int tid) {
+    const int my_slot = (crank == 0) ? 1 : parity;
+    const int n_el = w * rpad;
+    double2 *mine = X + (size_t)my_slot * wmax * rpad;
+    double2 *their_stage = cluster.map_shared_rank(stage, crank ^ 1);
+    cluster.sync();  // partner finished its rounds and its previous staging copy
+    for (int e = tid; e < n_el; e += kUpdThreads) their_stage[e] = mine[e];
+    cluster.sync();  // both staging areas filled
+    for (int e = tid; e < n_el; e += kUpdThreads) mine[e] = stage[e];
+    __syncthreads();
+}
+
+template <int RPL>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kUpdThreads, 1)
+    update2q_fp64_kernel(const Upd2Params p) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
+    const int pi = (int)(blockIdx.x >> 1);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CtaScalars *sc = reinterpret_cast<CtaScalars *>(smem_raw);
+    const int wmax = p.wmax, rpad = p.rpad;
+    double2 *X = reinterpret_cast<double2 *>(smem_raw + 384);
+    double2 *stage = X + (size_t)2 * wmax * rpad;
+    double *sig2 = reinterpret_cast<double *>(stage + (size_t)wmax * rpad);
+    double *Ssorted = sig2 + 2 * wmax;
+    int *rank = reinterpret_cast<int *>(Ssorted + 4 * wmax);
+    int *klist = rank + 2 * wmax;
+
+    const mpsb_pair pr = p.pairs[pi];
+    const mpsb_chain ch = p.chains[pr.chain];
+    const int i = pr.site;
+    bool bad = (i < 0) || (i + 2 > ch.n);
+    int cl = 0, cm = 0, cr = 0;
+    if (!bad) {
+        cl = ch.bonds[i];
+        cm = ch.bonds[i + 1];
+        cr = ch.bonds[i + 2];
+        bad = cl < 1 || cm < 1 || cr < 1 || cl > p.chi_cap || cm > p.chi_cap || cr > p.chi_cap ||
+              ch.chi_max < 1 || ch.chi_max > p.chi_cap;
+    }
+    if (bad) {  // both CTAs see the same data and leave together
+        if (crank == 0 && tid == 0) {
+            p.rec[pi] = PairRec{0.0, 0.0, 0.0, cm, MPSB_ST_BADDIM};
+            p.status[pr.out] = MPSB_ST_BADDIM;
+            if (p.kept) p.kept[pr.out] = cm;
+            if (p.trunc) p.trunc[pr.out] = 0.0;
+        }
+        return;
+    }
+
+    const bool trans = cr > cl;  // Jacobi on M^H when M is wide
+    const int R = trans ? 2 * cr : 2 * cl;
+    const int C = trans ? 2 * cl : 2 * cr;
+    const int D = C >> 1;
+    const int w = ((C + 7) & ~7) >> 2;
+    const int idx0 = crank * w;
+    const int nidx = max(0, min(D, idx0 + w) - idx0);
+
+    for (int e = tid; e < 2 * wmax * rpad; e += kUpdThreads) X[e] = make_double2(0.0, 0.0);
+    if (tid == 0) {
+        sc->nrot[0] = 0;
+        sc->nrot[1] = 0;
+        sc->nonfinite = 0;
+    }
+    if (tid < 16) sc->gate[tid] = __ldg(p.gates + (size_t)pr.gate * 16 + tid);
+    __syncthreads();
+
+    // ---- phase 1: theta for this CTA's columns, into X (smem) and X0 (workspace)
+    {
+        const double2 *g = sc->gate;
+        const double2 *A = reinterpret_cast<const double2 *>(ch.sites + (size_t)i * ch.slot_elems);
+        const double2 *B = reinterpret_cast<const double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
+        double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
+        const int other = trans ? cr : cl;
+        const int total = nidx * other;
+        int nonfin = 0;
+        for (int e = tid; e < total; e += kUpdThreads) {
+            int a, d;
+            if (!trans) {
+                a = e / nidx;
+                d = idx0 + (e - a * nidx);
+            } else {
+                const int q = e / cr;
+                a = idx0 + q;
+                d = e - q * cr;
+            }
+            double2 t00 = make_double2(0, 0), t01 = t00, t10 = t00, t11 = t00;
+            const double2 *ap0 = A + (size_t)(2 * a) * cm;
+            const double2 *ap1 = ap0 + cm;
+            const double2 *bp = B + d;
+            for (int b = 0; b < cm; ++b) {
+                const double2 a0 = __ldg(ap0 + b), a1 = __ldg(ap1 + b);
+                const double2 b0 = __ldg(bp + (size_t)(2 * b) * cr), b1 = __ldg(bp + (size_t)(2 * b + 1) * cr);
+                t00 = c_fma(a0, b0, t00);
+                t01 = c_fma(a0, b1, t01);
+                t10 = c_fma(a1, b0, t10);
+                t11 = c_fma(a1, b1, t11);
+            }
+#pragma unroll
+            for (int s0 = 0; s0 < 2; ++s0) {
+#pragma unroll
+                for (int s1 = 0; s1 < 2; ++s1) {
+                    const int s = 2 * s0 + s1;
+                    double2 m = c_mul(g[4 * s + 0], t00);
+                    m = c_fma(g[4 * s + 1], t01, m);
+                    m = c_fma(g[4 * s + 2], t10, m);
+                    m = c_fma(g[4 * s + 3], t11, m);
+                    nonfin |= !c_finite(m);
+                    if (!trans) {
+                        const int r = 2 * a + s0, j = 2 * (d - idx0) + s1;
+                        const int slot = j >= w, jj = j - slot * w;
+                        X[(size_t)(slot * wmax + jj) * rpad + r] = m;
+                        x0[(size_t)r * C + s1 * cr + d] = m;
+                    } else {
+                        const int r = s1 * cr + d, j = 2 * (a - idx0) + s0;
+                        const int slot = j >= w, jj = j - slot * w;
+                        const double2 mc = c_conj(m);
+                        X[(size_t)(slot * wmax + jj) * rpad + r] = mc;
+                        x0[(size_t)r * C + 2 * a + s0] = mc;
+                    }
+                }
+            }
+        }
+        if (nonfin) atomicOr(&sc->nonfinite, 1);
+        __threadfence();
+    }
+    __syncthreads();
+
+    // ---- phase 2: one-sided Jacobi sweeps over the cluster
+    int parity = 0;
+    bool converged = false;
+    for (int sweep = 0; sweep < p.max_sweeps; ++sweep) {
+        const int sb = sweep & 1;
+        if (tid == 0) sc->nrot[sb] = 0;
+        __syncthreads();
+        int cnt = 0;
+        for (int step = 0; step < 3; ++step) {
+            step_rounds<RPL>(X, w, wmax, rpad, step == 0, warp, lane, p.tol2, cnt);
+            if (step == 2 && lane == 0 && cnt) atomicAdd(&sc->nrot[sb], cnt);
+            exchange_slots(cluster, X, stage, crank, parity, w, wmax, rpad, tid);
+            parity ^= 1;
+        }
+        const int remote = *cluster.map_shared_rank(&sc->nrot[sb], crank ^ 1);
+        if (sc->nrot[sb] + remote == 0) {
+            converged = true;
+            break;
+        }
+    }
+
+    // ---- phase 3: singular values, ranks, keep rule
+    for (int j = warp; j < 2 * w; j += kUpdWarps) {
+        const int slot = j >= w, jj = j - slot * w;
+        const double2 *cp = X + (size_t)(slot * wmax + jj) * rpad;
+        double s = 0.0;
+#pragma unroll
+        for (int r = 0; r < RPL; ++r) s += c_abs2(cp[lane + 32 * r]);
+        s = warp_sum(s);
+        if (lane == 0) sig2[j] = s;
+    }
+    cluster.sync();  // (A) both sig2 arrays complete
+    {
+        const double *rsig2 = cluster.map_shared_rank(sig2, crank ^ 1);
+        double *rS = cluster.map_shared_rank(Ssorted, crank ^ 1);
+        const int base_me = crank * 2 * w, base_ot = (crank ^ 1) * 2 * w;
+        for (int j = tid; j < 2 * w; j += kUpdThreads) {
+            const double me = sig2[j];
+            const int gid = base_me + j;
+            int rk = 0;
+            for (int k = 0; k < 2 * w; ++k) {
+                const double o = sig2[k];
+                rk += (o > me) || (o == me && base_me + k < gid);
+            }
+            for (int k = 0; k < 2 * w; ++k) {
+                const double o = rsig2[k];
+                rk += (o > me) || (o == me && base_ot + k < gid);
+            }
+            rank[j] = rk;
+            const double sv = sqrt(me);
+            Ssorted[rk] = sv;
+            rS[rk] = sv;
+        }
+    }
+    int remote_nonfinite = 0;
+    if (tid == 0) remote_nonfinite = *cluster.map_shared_rank(&sc->nonfinite, crank ^ 1);
+    cluster.sync();  // (B) sorted spectrum complete in both CTAs
+
+    if (tid == 0) {
+        const double thr = ch.cutoff * Ssorted[0];
+        int cnt = 0;
+        double tot = 0.0;
+        for (int k = 0; k < C; ++k) {
+            const double v = Ssorted[k];
+            cnt += (v > thr);
+            tot = fma(v, v, tot);
+        }
+        const int keep = min(max(cnt, 1), ch.chi_max);
+        double dropped = 0.0;
+        for (int k = keep; k < C; ++k) dropped = fma(Ssorted[k], Ssorted[k], dropped);
+        double d1 = 0.0;
+        if (keep < C && dropped > 0.0) d1 = 0.5 * log(1.0 - dropped / fmax(tot, 1e-300));
+        double nk2 = 0.0;
+        for (int k = 0; k < keep; ++k) nk2 = fma(Ssorted[k], Ssorted[k], nk2);
+        const double nrm = sqrt(nk2);
+        double d2 = 0.0, div = 1.0;
+        if (nrm > 1e-15) {
+            d2 = log(nrm);
+            div = nrm;
+        }
+        sc->keep = keep;
+        sc->div = div;
+        int nk = 0;
+        for (int j = 0; j < 2 * w; ++j)
+            if (rank[j] < keep) klist[nk++] = j;
+        sc->nk = nk;
+        if (crank == 0) {
+            int st = converged ? 0 : MPSB_ST_NOCONV;
+            if (sc->nonfinite | remote_nonfinite) st |= MPSB_ST_NONFINITE;
+            const double disc = tot > 0.0 ? dropped / tot : 0.0;
+            p.rec[pi] = PairRec{d1, d2, disc, keep, st};
+            p.status[pr.out] = st;
+            if (p.kept) p.kept[pr.out] = keep;
+            if (p.trunc) p.trunc[pr.out] = disc;
+        }
+    }
+    __syncthreads();
+    if (crank == 0 && p.spectra) {
+        for (int j = tid; j < 128; j += kUpdThreads) p.spectra[(size_t)pr.out * 128 + j] = j < C ? Ssorted[j] : 0.0;
+    }
+
+    // ---- phase 4: write U sqrt(S) and sqrt(S) Vh into the two site slots
+    const int K = sc->keep, nk = sc->nk;
+    const double div = sc->div;
+    double2 *Aout = reinterpret_cast<double2 *>(ch.sites + (size_t)i * ch.slot_elems);
+    double2 *Bout = reinterpret_cast<double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
+    auto colp = [&](int j) {
+        const int slot = j >= w, jj = j - slot * w;
+        return X + (size_t)(slot * wmax + jj) * rpad;
+    };
+    // direct side: the vectors the Jacobi produced
+    for (int e = tid; e < nk * R; e += kUpdThreads) {
+        const int kk = e / R, r = e - kk * R;
+        const int j = klist[kk], rho = rank[j];
+        const double sg = Ssorted[rho];
+        const double f = sg > 0.0 ? sqrt(sg / div) / sg : 0.0;
+        const double2 v = colp(j)[r];
+        if (!trans)
+            Aout[(size_t)r * K + rho] = c_scale(v, f);
+        else
+            Bout[(size_t)rho * R + r] = c_scale(c_conj(v), f);
+    }
+    // other side: Y[rho, col] = sum_r conj(x_j[r]) X0[r, col]
+    {
+        const double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
+        const int col = tid & 127, grp = tid >> 7;
+        if (col < C) {
+            for (int base = grp * 8; base < nk; base += 32) {
+                const int nb = min(8, nk - base);
+                const double2 *cpk[8];
+                double2 acc[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    cpk[q] = colp(klist[base + (q < nb ? q : 0)]);
+                    acc[q] = make_double2(0.0, 0.0);
+                }
+                for (int r = 0; r < R; ++r) {
+                    const double2 xv = __ldcg(x0 + (size_t)r * C + col);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) acc[q] = c_cfma(cpk[q][r], xv, acc[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if (q < nb) {
+                        const int rho = rank[klist[base + q]];
+                        const double sg = Ssorted[rho];
+                        const double f = sg > 0.0 ? sqrt(sg / div) / (sg * sg) : 0.0;
+                        if (!trans)
+                            Bout[(size_t)rho * C + col] = c_scale(acc[q], f);
+                        else
+                            Aout[(size_t)col * K + rho] = c_scale(c_conj(acc[q]), f);
+                    }
+                }
+            }
+        }
+    }
+    if (crank == 0 && tid == 0) ch.bonds[i + 1] = K;
+    cluster.sync();
+}
+
+// Fold per-pair norm_log increments into each chain, in pair order
+// (norm_log += d_trunc; norm_log += d_norm, as mps_core.py:287-298 does), and
+// OR the pair statuses into the chain's status accumulator.
+__global__ void fold_norm_log_kernel(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+                                     const PairRec *rec) {
+    const int q0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q0 >= npairs) return;
+    const int c = pairs[q0].chain;
+    if (q0 > 0 && pairs[q0 - 1].chain == c) return;  // not the head of this chain's run
+    double *nl = chains[c].norm_log;
+    double acc = *nl;
+    int st = 0;
+    for (int q = q0; q < npairs && pairs[q].chain == c; ++q) {
+        acc += rec[q].d_trunc;
+        acc += rec[q].d_norm;
+        st |= rec[q].status;
+    }
+    *nl = acc;
+    if (chains[c].status_acc && st) atomicOr(chains[c].status_acc, st);
+}
+
+// ------------------------------------------------------------------ host
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+size_t upd_workspace_bytes(int npairs, int chi_cap) {
+    const size_t x0_stride = (size_t)(2 * chi_cap) * (2 * chi_cap);
+    return align256((size_t)npairs * sizeof(PairRec)) + (size_t)npairs * x0_stride * sizeof(double2);
+}
+
+template <int RPL>
+static int launch_rpl(const Upd2Params &p, size_t smem, cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        if (cudaFuncSetAttribute(update2q_fp64_kernel<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return check_launch("cudaFuncSetAttribute(update2q)");
+        configured = true;
+    }
+    update2q_fp64_kernel<RPL><<<2 * p.npairs, kUpdThreads, smem, s>>>(p);
+    return check_launch("update2q_fp64_kernel");
+}
+
+int launch_update2q(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const double2 *gates,
+                    int chi_cap, double tol, int max_sweeps, void *ws, double *spectra, int32_t *kept,
+                    double *trunc, int32_t *status, cudaStream_t stream) {
+    if (npairs == 0) return MPSB_OK;
+    Upd2Params p;
+    p.chains = chains;
+    p.pairs = pairs;
+    p.npairs = npairs;
+    p.gates = gates;
+    p.rec = reinterpret_cast<PairRec *>(ws);
+    p.x0 = reinterpret_cast<double2 *>(static_cast<char *>(ws) + align256((size_t)npairs * sizeof(PairRec)));
+    p.x0_stride = (long long)(2 * chi_cap) * (2 * chi_cap);
+    p.spectra = spectra;
+    p.kept = kept;
+    p.trunc = trunc;
+    p.status = status;
+    p.chi_cap = chi_cap;
+    const int rpl = (2 * chi_cap + 31) / 32;
+    p.rpad = 32 * rpl;
+    p.wmax = (((2 * chi_cap) + 7) & ~7) / 4;
+    p.tol2 = tol * tol;
+    p.max_sweeps = max_sweeps;
+    const size_t smem = upd_smem_bytes(p.wmax, p.rpad);
+    int rc;
+    switch (rpl) {
+        case 1: rc = launch_rpl<1>(p, smem, stream); break;
+        case 2: rc = launch_rpl<2>(p, smem, stream); break;
+        case 3: rc = launch_rpl<3>(p, smem, stream); break;
+        default: rc = launch_rpl<4>(p, smem, stream); break;
+    }
+    if (rc != MPSB_OK) return rc;
+    fold_norm_log_kernel<<<(npairs + 127) / 128, 128, 0, stream>>>(chains, pairs, npairs, p.rec);
+    return check_launch("fold_norm_log_kernel");
+}
+
+}  // namespace mpsb

@@ -1,0 +1,525 @@
+"""Device-resident MPS chains driven through libmpsb200 (no CPU fallback).
+
+``MPSState`` mirrors the public surface of the reference class
+``MPSState`` (mps_core.py:172-494): same constructor arguments, ``sites``,
+``norm_log``, ``apply_1q``, ``apply_2q``, ``_apply_adjacent_2q``,
+``get_statevector``, ``chi_l``/``chi_r``/``max_bond``/``bond_dims``,
+``copy``.  It adds what the reference lacks for long chains --
+``expectation``, ``amplitude`` and batched ``apply_layer`` -- with semantics
+fixed by the reference's statevector convention (amplitudes carry
+exp(norm_log); expectation values are normalised by <psi|psi>).
+
+``MPSBatch`` holds many independent chains of uneven length and bond cap in
+one allocation and advances them together, one launch per layer.
+
+Storage (HBM): every site owns a slot of 2*chi_cap^2 complex128; site k is
+kept C-order as (bonds[k], 2, bonds[k+1]) at the slot start.  Bond dimensions
+live on the device and are written by the update kernel, so a sequence of
+updates needs no host synchronisation.  Numerical faults (Jacobi not
+converged, non-finite theta) are OR-ed into a per-chain device word that the
+host checks whenever it reads results back (``check_status``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from typing import Dict, Iterable, List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+import torch
+
+from . import _lib
+from .gates import GATE_MATRICES, permute_2q
+
+__all__ = ["MPSState", "MPSBatch", "PairBatch", "PRECISIONS", "validate_pairs"]
+
+PRECISIONS = {"fp64": _lib.FP64, "complex128": _lib.FP64, "mixed": _lib.MIXED_TF32X3,
+              "tf32x3": _lib.MIXED_TF32X3}
+_SWAP = GATE_MATRICES["swap"]
+
+
+def _stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def validate_pairs(ns: Sequence[int], chain_idx: np.ndarray, sites: np.ndarray) -> None:
+    """Host check of one launch's pair table (the kernels trust it).
+
+    Every pair (i, i+1) must lie inside its chain, the pairs of a chain must
+    be disjoint, and all pairs of a chain must be contiguous in the table
+    (the per-chain norm_log fold walks one contiguous run).
+    """
+    chain_idx = np.asarray(chain_idx, np.int64)
+    sites = np.asarray(sites, np.int64)
+    if len(chain_idx) != len(sites):
+        raise ValueError("chain_idx and sites differ in length")
+    if len(chain_idx) == 0:
+        return
+    if np.any(chain_idx < 0) or np.any(chain_idx >= len(ns)):
+        raise ValueError("pair chain index out of range")
+    nn = np.asarray(ns, np.int64)[chain_idx]
+    if np.any(sites < 0) or np.any(sites + 1 >= nn):
+        raise ValueError("pair site out of range: need 0 <= i and i + 1 < n")
+    change = np.flatnonzero(np.diff(chain_idx) != 0)
+    heads = chain_idx[np.concatenate([[0], change + 1])]
+    if len(np.unique(heads)) != len(heads):
+        raise ValueError("all pairs of one chain must be contiguous in the batch")
+    order = np.lexsort((sites, chain_idx))
+    cs, ss = chain_idx[order], sites[order]
+    same = cs[1:] == cs[:-1]
+    if np.any(same & (ss[1:] - ss[:-1] < 2)):
+        raise ValueError("pairs of one launch must be disjoint")
+
+
+class _Workspace:
+    """Grow-only device scratch shared by the calls of one owner."""
+
+    def __init__(self, device):
+        self.device = device
+        self.buf: Optional[torch.Tensor] = None
+
+    def get(self, nbytes: int) -> torch.Tensor:
+        if self.buf is None or self.buf.numel() < nbytes:
+            self.buf = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+        return self.buf
+
+
+class PairBatch:
+    """Device descriptor table for one launch of disjoint two-site updates.
+
+    Built once on the host (validated: pairs in range, disjoint per chain,
+    chains contiguous) and reusable across launches and CUDA-graph replays.
+    """
+
+    def __init__(self, owner: "MPSBatch", chain_idx: Sequence[int], sites: Sequence[int],
+                 gates: np.ndarray, record_spectra: bool = False):
+        chain_idx = np.asarray(chain_idx, dtype=np.int32)
+        sites = np.asarray(sites, dtype=np.int32)
+        if isinstance(gates, torch.Tensor):
+            if gates.dtype != torch.complex128:
+                raise ValueError("gates must be complex128")
+            gates = gates.reshape(-1, 4, 4)
+        else:
+            gates = np.asarray(gates, dtype=np.complex128).reshape(-1, 4, 4)
+        if not (len(chain_idx) == len(sites) == len(gates)):
+            raise ValueError("chain_idx, sites and gates must have one entry per pair")
+        owner._validate_pairs(chain_idx, sites)
+        P = len(sites)
+        self.npairs = P
+        self.owner = owner
+        dev = owner.device
+        table = np.stack([chain_idx, sites, np.arange(P, dtype=np.int32), np.arange(P, dtype=np.int32)], 1)
+        self.pairs = torch.from_numpy(np.ascontiguousarray(table)).to(dev)
+        if isinstance(gates, torch.Tensor):  # e.g. pinned host memory: asynchronous copy
+            self.gates = gates.reshape(P, 16).to(dev, non_blocking=True)
+        else:
+            self.gates = torch.from_numpy(np.ascontiguousarray(gates.reshape(P, 16))).to(dev)
+        self.status = torch.zeros(P, dtype=torch.int32, device=dev)
+        self.kept = torch.zeros(P, dtype=torch.int32, device=dev)
+        self.trunc = torch.zeros(P, dtype=torch.float64, device=dev)
+        self.spectra = torch.zeros(P, 128, dtype=torch.float64, device=dev) if record_spectra else None
+
+    def set_gates(self, gates: np.ndarray) -> None:
+        g = torch.from_numpy(np.ascontiguousarray(np.asarray(gates, np.complex128).reshape(self.npairs, 16)))
+        self.gates.copy_(g, non_blocking=False)
+
+
+class MPSBatch:
+    """Independent chains in one device allocation.
+
+    ``ns[c]``, ``chi_maxs[c]``, ``cutoffs[c]`` give chain c's length, bond
+    cap and relative SVD cutoff.  All chains start in |0...0>.
+    """
+
+    def __init__(self, ns: Sequence[int], chi_maxs: Union[int, Sequence[int]] = 64,
+                 cutoffs: Union[float, Sequence[float]] = 1e-12, precision: str = "fp64",
+                 device: Union[str, torch.device] = "cuda", tol: float = 0.0, max_sweeps: int = 0):
+        self._lib = _lib.load()
+        ns = [int(v) for v in ns]
+        nch = len(ns)
+        chi_maxs = [int(chi_maxs)] * nch if np.isscalar(chi_maxs) else [int(v) for v in chi_maxs]
+        cutoffs = [float(cutoffs)] * nch if np.isscalar(cutoffs) else [float(v) for v in cutoffs]
+        if nch == 0 or len(chi_maxs) != nch or len(cutoffs) != nch:
+            raise ValueError("need one n, chi_max and cutoff per chain")
+        for n, chi in zip(ns, chi_maxs):
+            if n < 1:
+                raise ValueError(f"chain length must be >= 1, got {n}")
+            if not (1 <= chi <= _lib.MPSB_CHI_LIMIT):
+                raise ValueError(f"chi_max must be in [1, {_lib.MPSB_CHI_LIMIT}], got {chi}: the fused "
+                                 "kernel holds theta (<= 128 x 128) on chip")
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError("MPSBatch lives on a CUDA device; there is no CPU engine")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.precision = precision
+        self.tol = float(tol)
+        self.max_sweeps = int(max_sweeps)
+        self.ns = ns
+        self.chi_maxs = chi_maxs
+        self.cutoffs = cutoffs
+        self.chi_cap = max(chi_maxs)
+        self.slot = 2 * self.chi_cap * self.chi_cap
+        self.site_off = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
+        self.bond_off = self.site_off + np.arange(nch + 1)
+        dev = self.device
+        total = int(self.site_off[-1])
+        self.sites = torch.zeros(total, self.slot, dtype=torch.complex128, device=dev)
+        self.sites[:, 0] = 1.0
+        self.bonds = torch.ones(total + nch, dtype=torch.int32, device=dev)
+        self.norm_logs = torch.zeros(nch, dtype=torch.float64, device=dev)
+        self.status_acc = torch.zeros(nch, dtype=torch.int32, device=dev)
+        self._ws = _Workspace(dev)
+        self._ews = _Workspace(dev)
+        self._build_table()
+
+    # -- chain table ----------------------------------------------------------
+    def _build_table(self) -> None:
+        nch = len(self.ns)
+        arr = (_lib.Chain * nch)()
+        sb = self.sites.element_size() * self.slot
+        for c in range(nch):
+            arr[c].sites = self.sites.data_ptr() + int(self.site_off[c]) * sb
+            arr[c].bonds = self.bonds.data_ptr() + int(self.bond_off[c]) * 4
+            arr[c].norm_log = self.norm_logs.data_ptr() + c * 8
+            arr[c].status_acc = self.status_acc.data_ptr() + c * 4
+            arr[c].slot_elems = self.slot
+            arr[c].n = self.ns[c]
+            arr[c].chi_max = self.chi_maxs[c]
+            arr[c].cutoff = self.cutoffs[c]
+        raw = np.frombuffer(bytes(arr), dtype=np.uint8).copy()
+        self.table = torch.from_numpy(raw).to(self.device)
+        self._table_host = arr
+
+    def chain_ptr(self, c: int) -> int:
+        return self.table.data_ptr() + c * C.sizeof(_lib.Chain)
+
+    @property
+    def nchains(self) -> int:
+        return len(self.ns)
+
+    def _stream(self) -> int:
+        return _stream_handle(self.device)
+
+    def _validate_pairs(self, chain_idx: np.ndarray, sites: np.ndarray) -> None:
+        validate_pairs(self.ns, chain_idx, sites)
+
+    # -- updates --------------------------------------------------------------
+    def make_pairs(self, chain_idx, sites, gates, record_spectra: bool = False) -> PairBatch:
+        return PairBatch(self, chain_idx, sites, gates, record_spectra)
+
+    def run_pairs(self, pb: PairBatch, precision: Optional[str] = None) -> None:
+        """Launch one batched update (asynchronous, stream-ordered, graph-capturable)."""
+        if pb.npairs == 0:
+            return
+        prec = PRECISIONS[precision or self.precision]
+        need = self._lib.mpsb_update2q_workspace_bytes(pb.npairs, self.chi_cap)
+        ws = self._ws.get(need)
+        rc = self._lib.mpsb_update2q_batch(
+            self.table.data_ptr(), pb.pairs.data_ptr(), pb.npairs, pb.gates.data_ptr(), prec,
+            self.chi_cap, self.tol, self.max_sweeps, ws.data_ptr(), ws.numel(),
+            _ptr(pb.spectra), pb.kept.data_ptr(), pb.trunc.data_ptr(), pb.status.data_ptr(),
+            self._stream())
+        _lib.check(rc, "mpsb_update2q_batch")
+
+    def apply_layer(self, chain_idx, sites, gates, precision: Optional[str] = None,
+                    record_spectra: bool = False) -> PairBatch:
+        pb = self.make_pairs(chain_idx, sites, gates, record_spectra)
+        self.run_pairs(pb, precision)
+        return pb
+
+    def apply_1q_many(self, chain_idx, sites, gates) -> None:
+        chain_idx = np.asarray(chain_idx, np.int32)
+        sites = np.asarray(sites, np.int32)
+        g = np.asarray(gates, np.complex128).reshape(-1, 4)
+        if len(sites) == 0:
+            return
+        key = chain_idx.astype(np.int64) * (1 << 32) + sites
+        if len(np.unique(key)) != len(key):
+            raise ValueError("single-site ops of one launch must touch distinct sites")
+        if np.any(sites < 0) or np.any(sites >= np.asarray(self.ns)[chain_idx]):
+            raise ValueError("site out of range")
+        ops = np.stack([chain_idx, sites, np.arange(len(sites), dtype=np.int32),
+                        np.zeros(len(sites), np.int32)], 1)
+        ops_t = torch.from_numpy(np.ascontiguousarray(ops)).to(self.device)
+        g_t = torch.from_numpy(np.ascontiguousarray(g)).to(self.device)
+        rc = self._lib.mpsb_apply1q_batch(self.table.data_ptr(), ops_t.data_ptr(), len(sites),
+                                          g_t.data_ptr(), self.chi_cap, self._stream())
+        _lib.check(rc, "mpsb_apply1q_batch")
+
+    # -- read-out -------------------------------------------------------------
+    def check_status(self, raise_on_error: bool = True) -> np.ndarray:
+        st = self.status_acc.cpu().numpy()
+        if raise_on_error and np.any(st):
+            bad = {int(c): int(v) for c, v in enumerate(st) if v}
+            raise RuntimeError(f"two-site update reported numerical faults per chain {bad} "
+                               "(1 = Jacobi not converged, 2 = non-finite theta, 4 = bad bond dims)")
+        return st
+
+    def bond_dims(self, c: int = 0) -> List[int]:
+        b = self.bonds[int(self.bond_off[c]): int(self.bond_off[c]) + self.ns[c] + 1].cpu().numpy()
+        return [int(v) for v in b[1:-1]]
+
+    def norm_log(self, c: int = 0) -> float:
+        return float(self.norm_logs[c].item())
+
+    def site(self, c: int, k: int) -> np.ndarray:
+        b = self.bonds[int(self.bond_off[c]) + k: int(self.bond_off[c]) + k + 2].cpu().numpy()
+        flat = self.sites[int(self.site_off[c]) + k, : b[0] * 2 * b[1]].cpu().numpy()
+        return flat.reshape(int(b[0]), 2, int(b[1])).copy()
+
+    def set_site(self, c: int, k: int, tensor) -> None:
+        t = np.asarray(tensor, dtype=np.complex128)
+        if t.ndim != 3 or t.shape[1] != 2:
+            raise ValueError("site tensor must have shape (chi_l, 2, chi_r)")
+        n = self.ns[c]
+        bl, br = self.bonds[int(self.bond_off[c]) + k: int(self.bond_off[c]) + k + 2].cpu().numpy()
+        if (k == 0 and t.shape[0] != 1) or (k == n - 1 and t.shape[2] != 1):
+            raise ValueError("boundary bonds must be 1")
+        if max(t.shape[0], t.shape[2]) > self.chi_maxs[c]:
+            raise ValueError("bond dimension above chi_max")
+        # a bond can never exceed the Schmidt rank bound 2^min(left sites, right sites)
+        if t.shape[0] > 2 ** min(k, n - k) or t.shape[2] > 2 ** min(k + 1, n - k - 1):
+            raise ValueError("bond dimension above the Schmidt-rank bound of its cut")
+        row = torch.zeros(self.slot, dtype=torch.complex128)
+        row[: t.size] = torch.from_numpy(t.reshape(-1))
+        self.sites[int(self.site_off[c]) + k].copy_(row.to(self.device))
+        self.bonds[int(self.bond_off[c]) + k] = int(t.shape[0])
+        self.bonds[int(self.bond_off[c]) + k + 1] = int(t.shape[2])
+
+    def statevector(self, c: int = 0) -> np.ndarray:
+        n = self.ns[c]
+        if n > 24:
+            raise ValueError(f"Statevector reconstruction for n={n} > 24 not supported.")
+        out = torch.empty(1 << n, dtype=torch.complex128, device=self.device)
+        scratch = torch.empty(2 << n, dtype=torch.complex128, device=self.device)
+        rc = self._lib.mpsb_statevector(self.chain_ptr(c), n, self.chi_cap, out.data_ptr(), scratch.data_ptr(),
+                                        scratch.numel() * 16, self._stream())
+        _lib.check(rc, "mpsb_statevector")
+        return out.cpu().numpy()
+
+    def amplitudes(self, c: int, bits: np.ndarray, with_log: bool = False):
+        bits = np.ascontiguousarray(np.asarray(bits, dtype=np.uint8).reshape(-1, self.ns[c]))
+        nb = bits.shape[0]
+        bt = torch.from_numpy(bits).to(self.device)
+        out = torch.empty(nb, dtype=torch.complex128, device=self.device)
+        la = torch.empty(nb, dtype=torch.float64, device=self.device)
+        rc = self._lib.mpsb_amplitude(self.table.data_ptr(), c, self.ns[c], bt.data_ptr(), nb, self.chi_cap,
+                                      out.data_ptr(), la.data_ptr(), self._stream())
+        _lib.check(rc, "mpsb_amplitude")
+        return (out.cpu().numpy(), la.cpu().numpy()) if with_log else out.cpu().numpy()
+
+    def expect_terms(self, terms: Sequence[Tuple[int, np.ndarray, Optional[np.ndarray]]],
+                     chains: Optional[Sequence[int]] = None) -> np.ndarray:
+        """Normalised <O> for terms (site, O_site, O_next or None) on chains 0..nchains-1.
+
+        All chains evaluated together must have the same length; returns
+        (nchains, nterms).
+        """
+        nch = self.nchains if chains is None else len(chains)
+        if chains is not None and list(chains) != list(range(nch)):
+            raise ValueError("expect_terms evaluates a leading range of chains")
+        n = self.ns[0]
+        if any(self.ns[c] != n for c in range(nch)):
+            raise ValueError("chains evaluated together must have equal length")
+        sites = np.array([t[0] for t in terms], np.int32)
+        two = np.array([0 if t[2] is None else 1 for t in terms], np.int32)
+        if np.any(sites < 0) or np.any(sites + two >= n):
+            raise ValueError("term site out of range")
+        ops = np.zeros((len(terms), 2, 4), np.complex128)
+        for k, (_, o1, o2) in enumerate(terms):
+            ops[k, 0] = np.asarray(o1, np.complex128).reshape(4)
+            ops[k, 1] = np.eye(2).reshape(4) if o2 is None else np.asarray(o2, np.complex128).reshape(4)
+        dev = self.device
+        st, tt, ot = (torch.from_numpy(sites).to(dev), torch.from_numpy(two).to(dev),
+                      torch.from_numpy(ops.reshape(-1)).to(dev))
+        out = torch.empty(nch * len(terms), dtype=torch.float64, device=dev)
+        need = self._lib.mpsb_expect_workspace_bytes(nch, n, self.chi_cap)
+        ws = self._ews.get(need)
+        rc = self._lib.mpsb_expect_local(self.table.data_ptr(), nch, n, self.chi_cap, st.data_ptr(),
+                                         tt.data_ptr(), ot.data_ptr(), len(terms), out.data_ptr(),
+                                         ws.data_ptr(), ws.numel(), self._stream())
+        _lib.check(rc, "mpsb_expect_local")
+        return out.cpu().numpy().reshape(nch, len(terms))
+
+
+_PAULI = {"I": np.eye(2, dtype=np.complex128), "X": GATE_MATRICES["x"], "Y": GATE_MATRICES["y"],
+          "Z": GATE_MATRICES["z"]}
+
+
+class _SitesView:
+    """List-like access to the device site tensors: host copies on read, uploads on write."""
+
+    def __init__(self, st: "MPSState"):
+        self._st = st
+
+    def __len__(self):
+        return self._st.n
+
+    def __getitem__(self, k):
+        if isinstance(k, slice):
+            return [self[j] for j in range(*k.indices(len(self)))]
+        if k < 0:
+            k += len(self)
+        if not 0 <= k < len(self):
+            raise IndexError(k)
+        return self._st._b.site(0, k)
+
+    def __setitem__(self, k, value):
+        self._st._b.set_site(0, k, value)
+
+    def __iter__(self):
+        return (self[k] for k in range(len(self)))
+
+
+class MPSState:
+    """One MPS chain on the GPU with the reference class's interface.
+
+    Parameters follow mps_core.MPSState(n, chi_max, svd_cutoff); ``chi_max``
+    is capped at 64 (the FPGA build of the reference caps it the same way,
+    fpga_mps_simulator.py:80-85).  ``precision`` selects the FP64 drop-in form
+    or the mixed 3xTF32 form.
+    """
+
+    def __init__(self, n: int, chi_max: int = 64, svd_cutoff: float = 1e-12, precision: str = "fp64",
+                 device: Union[str, torch.device] = "cuda", tol: float = 0.0, max_sweeps: int = 0):
+        self.n = int(n)
+        self.chi_max = int(chi_max)
+        self.svd_cutoff = float(svd_cutoff)
+        self._b = MPSBatch([self.n], [self.chi_max], [self.svd_cutoff], precision, device, tol, max_sweeps)
+        self.precision = precision
+        self._one = {}
+        self.last_pairs: Optional[PairBatch] = None
+
+    @property
+    def device(self) -> torch.device:
+        return self._b.device
+
+    # -- state -------------------------------------------------------------
+    @property
+    def sites(self) -> _SitesView:
+        return _SitesView(self)
+
+    @sites.setter
+    def sites(self, tensors) -> None:
+        tensors = list(tensors)
+        if len(tensors) != self.n:
+            raise ValueError("need one tensor per site")
+        for k, t in enumerate(tensors):
+            self._b.set_site(0, k, t)
+
+    @property
+    def norm_log(self) -> float:
+        return self._b.norm_log(0)
+
+    @norm_log.setter
+    def norm_log(self, value: float) -> None:
+        self._b.norm_logs[0] = float(value)
+
+    def copy(self) -> "MPSState":
+        out = MPSState(self.n, self.chi_max, self.svd_cutoff, self.precision, self.device,
+                       self._b.tol, self._b.max_sweeps)
+        out._b.sites.copy_(self._b.sites)
+        out._b.bonds.copy_(self._b.bonds)
+        out._b.norm_logs.copy_(self._b.norm_logs)
+        out._b.status_acc.copy_(self._b.status_acc)
+        return out
+
+    def chi_l(self, i: int) -> int:
+        return 1 if i == 0 else self.bond_dims()[i - 1]
+
+    def chi_r(self, i: int) -> int:
+        return 1 if i == self.n - 1 else self.bond_dims()[i]
+
+    def bond_dims(self) -> List[int]:
+        return self._b.bond_dims(0)
+
+    def max_bond(self) -> int:
+        return max(self.bond_dims()) if self.n > 1 else 1
+
+    def check_status(self, raise_on_error: bool = True) -> int:
+        return int(self._b.check_status(raise_on_error)[0])
+
+    # -- gates -------------------------------------------------------------
+    def apply_1q(self, site: int, gate: np.ndarray) -> None:
+        """A'[l, s', r] = sum_s G[s', s] A[l, s, r] (mps_core.py:267-273)."""
+        self._b.apply_1q_many([0], [int(site)], np.asarray(gate, np.complex128).reshape(1, 2, 2))
+
+    def _apply_adjacent_2q(self, i: int, gate: np.ndarray) -> None:
+        """contract -> gate -> truncated SVD -> sqrt(S) split on (i, i+1) (mps_core.py:326-350)."""
+        self.last_pairs = self._b.apply_layer([0], [int(i)], np.asarray(gate, np.complex128).reshape(1, 4, 4))
+
+    apply_adjacent_2q = _apply_adjacent_2q
+
+    def apply_2q(self, i: int, j: int, gate: np.ndarray) -> None:
+        """Dispatch of mps_core.py:304-324, including its SWAP routing.
+
+        Non-adjacent (i, j) is routed with SWAPs and the gate applied on
+        (lo, lo+1) as given (the reference does not re-index it); an adjacent
+        pair given as (i+1, i) re-indexes the gate with [0, 2, 1, 3].
+        """
+        g = np.asarray(gate, np.complex128).reshape(4, 4)
+        if abs(i - j) != 1:
+            lo, hi = min(i, j), max(i, j)
+            for k in range(hi, lo + 1, -1):
+                self.apply_2q(k - 1, k, _SWAP)
+            self.apply_2q(lo, lo + 1, g)
+            for k in range(lo + 1, hi):
+                self.apply_2q(k, k + 1, _SWAP)
+            return
+        if i > j:
+            i, j = j, i
+            g = permute_2q(g)
+        self._apply_adjacent_2q(i, g)
+
+    def apply_layer(self, sites: Sequence[int], gates: np.ndarray, record_spectra: bool = False) -> PairBatch:
+        """All disjoint adjacent pairs (i, i+1), i in ``sites``, in one launch."""
+        self.last_pairs = self._b.apply_layer(np.zeros(len(sites), np.int32), sites, gates,
+                                              record_spectra=record_spectra)
+        return self.last_pairs
+
+    # -- read-out ------------------------------------------------------------
+    def get_statevector(self) -> np.ndarray:
+        """Dense amplitudes in Qiskit order including exp(norm_log) (mps_core.py:433-461)."""
+        self.check_status()
+        return self._b.statevector(0)
+
+    def amplitude(self, bits: Union[str, Sequence[int]]) -> complex:
+        """<b|psi> including exp(norm_log).  A string is read Qiskit-style (last char = qubit 0)."""
+        if isinstance(bits, str):
+            bits = [int(ch) for ch in reversed(bits)]
+        self.check_status()
+        return complex(self._b.amplitudes(0, np.asarray(bits)[None, :])[0])
+
+    def expectation(self, op: Union[str, Dict[int, np.ndarray]]) -> float:
+        """Normalised <psi|O|psi>/<psi|psi> for a local operator.
+
+        ``op`` is a Pauli string in Qiskit order (character k from the left
+        acts on qubit n-1-k, as _pauli_expectation_sv reads it,
+        fpga_mps_simulator.py:1091-1108) or a dict {site: 2x2 matrix}; the
+        non-identity part must sit on one site or two adjacent sites.
+        """
+        if isinstance(op, str):
+            if len(op) != self.n:
+                raise ValueError("Pauli string length must equal n")
+            op = {self.n - 1 - k: _PAULI[ch.upper()] for k, ch in enumerate(op) if ch.upper() != "I"}
+        if not op:
+            return 1.0
+        ks = sorted(op)
+        if len(ks) > 2 or (len(ks) == 2 and ks[1] != ks[0] + 1):
+            raise ValueError("expectation supports one site or two adjacent sites")
+        self.check_status()
+        term = (ks[0], op[ks[0]], op[ks[1]] if len(ks) == 2 else None)
+        return float(self._b.expect_terms([term])[0, 0])
+
+    def expect_z_all(self) -> np.ndarray:
+        return self._b.expect_terms([(k, _PAULI["Z"], None) for k in range(self.n)])[0]
+
+    def expect_terms(self, terms) -> np.ndarray:
+        return self._b.expect_terms(terms)[0]

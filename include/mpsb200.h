@@ -1,0 +1,170 @@
+/*
+ * mpsb200.h -- C ABI of the B200 (sm_100a) MPS two-site update library
+ * (libmpsb200.so).
+ *
+ * Plain C: pointers, sizes, enums.  Every pointer marked "device" is CUDA
+ * device memory owned by the caller; the library never allocates or frees
+ * caller memory and keeps no per-call global state.  Every call is
+ * stream-ordered and asynchronous on the given stream (no host sync inside)
+ * unless its comment says otherwise.  Return value: MPSB_OK (0) or a negative
+ * MPSB_E* code; mpsb_last_error() then holds a message for this host thread.
+ * Numerical faults of individual pairs (no Jacobi convergence, non-finite
+ * theta, bad bond dimensions) are reported per pair in `status`.
+ *
+ * Reference interfaces replaced (paths within nasir26/fpga-mps-simulator):
+ *   mps_core.py:326-350   MPSState._apply_adjacent_2q  (contract -> gate -> SVD -> split)
+ *   mps_core.py:277-300   MPSState._svd_truncate       (keep rule, renormalise, norm_log)
+ *   fpga_mps_simulator.cpp:287-371 contract_and_apply_2q (the FPGA-offloaded contraction)
+ *   fpga_mps_simulator.cpp:392-404 fpga_mps_simulator   (the FPGA kernel entry point)
+ *   fpga_mps_simulator.py:566-635  2-qubit branch of _run_circuit_fpga (launch + host SVD)
+ */
+#ifndef MPSB200_H
+#define MPSB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define MPSB_API __attribute__((visibility("default")))
+#else
+#define MPSB_API
+#endif
+
+struct CUstream_st;
+typedef struct CUstream_st *mpsb_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+/* complex128, interleaved (re, im) -- the layout of numpy/torch complex128. */
+typedef struct { double re, im; } mpsb_c128;
+
+/* Largest bond dimension the kernels support (theta is at most 128 x 128). */
+#define MPSB_CHI_LIMIT 64
+
+/* One MPS chain resident in device memory (the state of mps_core.py:172-195).
+ * Site k is stored C-order as (bonds[k], 2, bonds[k+1]) complex128 at the
+ * start of its slot: sites + k * slot_elems.  bonds[0] = bonds[n] = 1.      */
+typedef struct {
+    mpsb_c128 *sites;      /* device: n * slot_elems complex128                  */
+    int32_t   *bonds;      /* device: n + 1 bond dimensions                      */
+    double    *norm_log;   /* device: one double, accumulated log-norm           */
+    int32_t   *status_acc; /* device: OR of every pair status of this chain, or NULL */
+    int64_t    slot_elems; /* complex elements per slot, >= 2 * chi_max^2       */
+    int32_t    n;          /* number of sites                                    */
+    int32_t    chi_max;    /* truncation cap, 1 .. MPSB_CHI_LIMIT               */
+    double     cutoff;     /* relative singular-value cutoff (svd_cutoff)       */
+} mpsb_chain;
+
+/* One two-site update: gate `gate` on sites (site, site + 1) of chain `chain`.
+ * Pairs of one call must be disjoint, and all pairs of one chain must be
+ * contiguous in the array (norm_log is folded per contiguous run, in order). */
+typedef struct {
+    int32_t chain;  /* index into the chain table                          */
+    int32_t site;   /* left site i of the pair (i, i + 1)                   */
+    int32_t gate;   /* index into the gate array (16 complex128, row-major) */
+    int32_t out;    /* row of this pair in status / kept / trunc / spectra  */
+} mpsb_pair;
+
+/* One single-site gate: 2x2 gate `gate` on site `site` of chain `chain`. */
+typedef struct {
+    int32_t chain;
+    int32_t site;
+    int32_t gate;   /* index into the gate array (4 complex128, row-major) */
+    int32_t pad;
+} mpsb_site_op;
+
+enum mpsb_precision {
+    MPSB_FP64 = 0,        /* complex128 end to end (the drop-in form)                    */
+    MPSB_MIXED_TF32X3 = 1 /* theta by 3xTF32 complex-3M tensor-core GEMMs; FP64 SVD       */
+};
+
+enum mpsb_status_bits {
+    MPSB_ST_OK = 0,
+    MPSB_ST_NOCONV = 1,    /* Jacobi hit max_sweeps; result written anyway */
+    MPSB_ST_NONFINITE = 2, /* theta held NaN or Inf                         */
+    MPSB_ST_BADDIM = 4     /* bond dimensions out of range; pair skipped    */
+};
+
+enum mpsb_error {
+    MPSB_OK = 0,
+    MPSB_EINVAL = -1,     /* bad argument (message in mpsb_last_error)  */
+    MPSB_ELAUNCH = -2,    /* CUDA launch / runtime error                */
+    MPSB_EWORKSPACE = -3, /* workspace too small                        */
+    MPSB_ENODEV = -4      /* no sm_100 device current                   */
+};
+
+/* Library version string and the last error message of the calling thread. */
+MPSB_API const char *mpsb_version(void);
+MPSB_API const char *mpsb_last_error(void);
+
+/* Bytes of device workspace mpsb_update2q_batch needs for `npairs` pairs
+ * whose bond dimensions never exceed chi_cap. */
+MPSB_API size_t mpsb_update2q_workspace_bytes(int npairs, int chi_cap);
+
+/* Batched two-site update (mps_core.py:326-350 + :277-300 for every pair).
+ * For each pair: theta = G . (A_i x A_{i+1}), M = theta as (2 chi_l) x (2 chi_r),
+ * truncated SVD with keep = clip(#(S > cutoff*S[0]), 1, chi_max), norm_log
+ * += 0.5 log(1 - dropped/total) when truncating, kept S renormalised to unit
+ * 2-norm (norm_log += log norm when norm > 1e-15), sites i and i+1 replaced by
+ * U sqrt(S) and sqrt(S) Vh in place, bonds[i+1] = keep.
+ *   chains, pairs, gates: device.  chi_cap: largest bond of any chain touched.
+ *   tol: Jacobi off-diagonal tolerance (<= 0 picks the form's default).
+ *   max_sweeps: Jacobi sweep bound (<= 0 picks 40).
+ *   spectra (nullable): npairs_out x 128 doubles, full descending spectrum.
+ *   kept, trunc (nullable): kept count and discarded weight dropped/total.
+ *   status (required): per-pair MPSB_ST_* bits.
+ * Replaces fpga_mps_simulator.py:566-635 (launch, read theta, host SVD, write back). */
+MPSB_API int mpsb_update2q_batch(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+                        const mpsb_c128 *gates, int precision, int chi_cap,
+                        double tol, int max_sweeps,
+                        void *workspace, size_t workspace_bytes,
+                        double *spectra, int32_t *kept, double *trunc, int32_t *status,
+                        mpsb_stream_t stream);
+
+/* Batched single-site gates, A'[l,s',r] = sum_s G[s',s] A[l,s,r], in place
+ * (mps_core.py:267-273; fpga_mps_simulator.cpp:232-276 apply_1q_gate).
+ * Ops of one call must touch distinct sites. */
+MPSB_API int mpsb_apply1q_batch(const mpsb_chain *chains, const mpsb_site_op *ops, int nops,
+                       const mpsb_c128 *gates, int chi_cap, mpsb_stream_t stream);
+
+/* Dense statevector of one chain (n <= 24) in Qiskit order, including
+ * exp(norm_log) (mps_core.py:433-461).  chain_dev: device pointer to the
+ * chain.  out: device, 2^n complex128.  scratch: device, 2 * 2^n complex128.
+ * Launches n + 1 kernels. */
+MPSB_API int mpsb_statevector(const mpsb_chain *chain_dev, int n, int chi_cap, mpsb_c128 *out,
+                     mpsb_c128 *scratch, size_t scratch_bytes, mpsb_stream_t stream);
+
+/* Amplitudes <b|psi> of `nbits` basis states of chain `chain` (b given as
+ * n bytes per state, byte k = value of qubit k), including exp(norm_log)
+ * (the convention of mps_core.py:433-461).  out: device complex128 per state;
+ * log_abs (nullable): log|amplitude| for chains where the value underflows. */
+MPSB_API int mpsb_amplitude(const mpsb_chain *chains, int chain, int n, const uint8_t *bits, int nbits,
+                   int chi_cap, mpsb_c128 *out, double *log_abs, mpsb_stream_t stream);
+
+/* Bytes of device scratch mpsb_expect_local needs for chains of n sites. */
+MPSB_API size_t mpsb_expect_workspace_bytes(int nchains, int n, int chi_cap);
+
+/* Normalised local expectation values <psi|O|psi>/<psi|psi> for `nterms`
+ * terms per chain, chains 0 .. nchains-1 of the table (all of length n).
+ * Term t acts with ops[2*t] on site sites[t] and, if two_site[t] != 0, with
+ * ops[2*t+1] on site sites[t]+1 (ops: device, 2x2 complex128 each).
+ * out: device, nchains x nterms doubles.  No reference counterpart: the
+ * semantics follow _pauli_expectation_sv (fpga_mps_simulator.py:1091-1108)
+ * applied to the statevector of mps_core.py:433-461, normalised. */
+MPSB_API int mpsb_expect_local(const mpsb_chain *chains, int nchains, int n, int chi_cap,
+                      const int32_t *sites, const int32_t *two_site, const mpsb_c128 *ops,
+                      int nterms, double *out, void *workspace, size_t workspace_bytes,
+                      mpsb_stream_t stream);
+
+/* FP64 FMA throughput probe: `blocks` x `threads` threads each run eight
+ * independent FMA chains of `iters` steps (16 * iters flops per thread).
+ * The caller times the launch on `stream` to state the FP64 roofline.
+ * sink: device, one double (written only to keep the chains live). */
+MPSB_API int mpsb_fp64_probe(int64_t iters, int blocks, int threads, double *sink, mpsb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPSB200_H */

@@ -1,0 +1,89 @@
+"""CPU baseline runner -- TEST/BENCH INFRASTRUCTURE ONLY.
+
+Times the oracle restatement of the reference engine (mps_core.py semantics,
+scipy gesdd SVD) on the host cores: one worker process per core, each pinned
+to one BLAS thread and advancing its own independent replica of the circuit,
+which is how the reference's per-update Python/LAPACK code parallelises
+across a CPU.  Workers are started with the "spawn" method so that no forked
+child inherits a CUDA context.
+"""
+from __future__ import annotations
+
+import math
+import multiprocessing as mp
+import os
+import time
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+
+def _haar(rng):
+    z = (rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4))) / math.sqrt(2.0)
+    q, r = np.linalg.qr(z)
+    d = np.diagonal(r)
+    return q * (d / np.abs(d))[None, :]
+
+
+def _circuit(n: int, depth: int, seed: int) -> List[Tuple[int, np.ndarray]]:
+    rng = np.random.default_rng(seed)
+    out = []
+    for layer in range(depth):
+        for i in range(layer % 2, n - 1, 2):
+            out.append((i, _haar(rng)))
+    return out
+
+
+def _worker(args) -> Tuple[int, float]:
+    n, depth, chi, cutoff, seed, reps = args
+    try:
+        from threadpoolctl import threadpool_limits
+        limiter = threadpool_limits(1)
+    except Exception:  # pragma: no cover
+        limiter = None
+    import sys
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if here not in sys.path:
+        sys.path.insert(0, here)
+    from oracle.mps_oracle import OracleMPS
+    gates = _circuit(n, depth, seed)
+    t0 = time.perf_counter()
+    count = 0
+    for _ in range(reps):
+        st = OracleMPS(n, chi, cutoff, record=False)
+        for i, g in gates:
+            st.apply_adjacent_2q(i, g)
+        count += len(gates)
+    dt = time.perf_counter() - t0
+    del limiter
+    return count, dt
+
+
+def usable_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:  # pragma: no cover
+        return os.cpu_count() or 1
+
+
+def run_parallel(n: int, depth: int, chi: int, cutoff: float, workers: int, reps: int = 1,
+                 seed: int = 0, pool=None) -> Dict[str, float]:
+    """Aggregate updates/s of `workers` single-threaded processes, each running `reps` circuits."""
+    own = pool is None
+    if own:
+        pool = mp.get_context("spawn").Pool(workers)
+    try:
+        t0 = time.perf_counter()
+        res = pool.map(_worker, [(n, depth, chi, cutoff, seed + w, reps) for w in range(workers)])
+        wall = time.perf_counter() - t0
+    finally:
+        if own:
+            pool.close()
+            pool.join()
+    updates = sum(r[0] for r in res)
+    return {"updates": updates, "wall_s": wall, "updates_per_s": updates / wall,
+            "per_worker_s": float(np.mean([r[1] for r in res])), "workers": workers}
+
+
+def make_pool(workers: int):
+    return mp.get_context("spawn").Pool(workers)

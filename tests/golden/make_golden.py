@@ -1,0 +1,205 @@
+"""Generate the golden fixtures in this folder by running the reference engine.
+
+Run from the repository root in a container where the reference checkout is
+mounted (read-only) at /root/reference:
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+It imports the reference's ``mps_core.py`` unchanged, drives it through its own
+public methods (``apply_1q``, ``apply_2q``, ``_apply_adjacent_2q``,
+``get_statevector``, ``get_counts``) and records what they return.  The
+per-update singular values are captured by wrapping ``la.svd`` inside the
+reference module, which leaves its numerics untouched.  Circuits come from the
+reference's own checks: the six small circuits of ``fpga_diag.py:28-58`` and
+the 3-qubit GHZ self-test of ``fpga_mps_simulator.py:1147-1165``, re-expressed
+as gate-list calls because Qiskit is not installed.
+
+The committed ``.npz`` files are what the tests read; this script is not run
+by the tests.
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+sys.path.insert(0, REF)
+import mps_core  # noqa: E402  (the reference module, unchanged)
+
+
+def haar(rng):
+    z = (rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4))) / math.sqrt(2.0)
+    q, r = np.linalg.qr(z)
+    d = np.diag(r)
+    return q * (d / np.abs(d))
+
+
+def brick(n, depth, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for layer in range(depth):
+        for i in range(layer % 2, n - 1, 2):
+            out.append((i, haar(rng)))
+    return out
+
+
+class Recorder:
+    """Wrap the reference module's SVD call to capture every spectrum."""
+
+    def __init__(self):
+        self.spectra = []
+        self._orig = mps_core.la.svd
+
+    def __enter__(self):
+        def svd(*a, **k):
+            u, s, vh = self._orig(*a, **k)
+            self.spectra.append(np.array(s, copy=True))
+            return u, s, vh
+        mps_core.la.svd = svd
+        return self
+
+    def __exit__(self, *exc):
+        mps_core.la.svd = self._orig
+
+
+def pack_spectra(spectra):
+    width = max(len(s) for s in spectra)
+    arr = np.zeros((len(spectra), width))
+    lens = np.zeros(len(spectra), dtype=np.int32)
+    for k, s in enumerate(spectra):
+        arr[k, :len(s)] = s
+        lens[k] = len(s)
+    return arr, lens
+
+
+def amplitudes(st, bit_rows):
+    out = []
+    for bits in bit_rows:
+        v = np.ones((1,), np.complex128)
+        for k in range(st.n):
+            v = v @ st.sites[k][:, int(bits[k]), :]
+        out.append(v[0] * math.exp(st.norm_log))
+    return np.array(out)
+
+
+def run_brick(name, n, depth, chi, cutoff, seed, n_amp=64, full_sv=False):
+    gates = brick(n, depth, seed)
+    st = mps_core.MPSState(n, chi, cutoff)
+    norm_logs, bonds = [], []
+    with Recorder() as rec:
+        for i, g in gates:
+            st._apply_adjacent_2q(i, g)
+            norm_logs.append(st.norm_log)
+            bonds.append(st.bond_dims())
+    spec, lens = pack_spectra(rec.spectra)
+    rng = np.random.default_rng(seed + 1)
+    bit_rows = rng.integers(0, 2, size=(n_amp, n))
+    bit_rows[0] = 0
+    data = dict(n=n, depth=depth, chi_max=chi, cutoff=cutoff, seed=seed,
+                sites=np.array([i for i, _ in gates], np.int32),
+                gates=np.stack([g for _, g in gates]),
+                spectra=spec, spec_len=lens, norm_log=np.array(norm_logs),
+                bonds=np.array(bonds, np.int32), bits=bit_rows.astype(np.int8),
+                amps=amplitudes(st, bit_rows))
+    if full_sv:
+        data["statevector"] = st.get_statevector()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **data)
+    print(name, "updates", len(gates), "max bond", st.max_bond(), "norm_log", st.norm_log)
+
+
+def run_gate_tables():
+    names_1q = sorted(mps_core._SINGLE_QUBIT_GATES)
+    names_2q = sorted(mps_core._TWO_QUBIT_GATES - {"cnot"})
+    params = [0.37, -1.21, 2.05]
+    g1 = np.stack([mps_core._gate_1q(nm, params) for nm in names_1q])
+    g2 = np.stack([mps_core._gate_2q(nm, params) for nm in names_2q])
+    np.savez_compressed(os.path.join(HERE, "gate_tables.npz"),
+                        names_1q=np.array(names_1q), names_2q=np.array(names_2q),
+                        params=np.array(params), g1=g1, g2=g2)
+
+
+def run_diag_circuits():
+    """fpga_diag.py:28-58 as mps_core gate-list calls, plus the GHZ-3 self-test."""
+    U = mps_core._gate_1q
+    G2 = mps_core._gate_2q
+    cases = {
+        "bell": (2, [("1", 0, U("h", None)), ("2", 0, 1, G2("cx", None))]),
+        "ghz4": (4, [("1", 0, U("h", None))] + [("2", i, i + 1, G2("cx", None)) for i in range(3)]),
+        "cx03": (4, [("1", 0, U("h", None)), ("2", 0, 3, G2("cx", None))]),
+        "u1": (1, [("1", 0, U("u", [0.7, 1.3, -0.4]))]),
+        "ucxu": (2, [("1", 0, U("u", [0.7, 1.3, -0.4])), ("1", 1, U("u", [-0.9, 0.2, 2.1])),
+                     ("2", 0, 1, G2("cx", None)), ("1", 0, U("u", [0.3, -0.6, 1.1]))]),
+        "ucx02": (4, [("1", 0, U("u", [0.7, 1.3, -0.4])), ("1", 2, U("u", [-0.9, 0.2, 2.1])),
+                      ("2", 0, 2, G2("cx", None))]),
+        "ghz3": (3, [("1", 0, U("h", None)), ("2", 0, 1, G2("cx", None)), ("2", 1, 2, G2("cx", None))]),
+    }
+    out = {}
+    for key, (n, ops) in cases.items():
+        st = mps_core.MPSState(n, 64, 1e-12)
+        enc = []
+        for op in ops:
+            if op[0] == "1":
+                st.apply_1q(op[1], op[2])
+                enc.append((1, op[1], -1, np.pad(op[2].reshape(-1), (0, 12))))
+            else:
+                st.apply_2q(op[1], op[2], op[3])
+                enc.append((2, op[1], op[2], op[3].reshape(-1)))
+        out[key + "_n"] = n
+        out[key + "_kind"] = np.array([e[0] for e in enc], np.int32)
+        out[key + "_qa"] = np.array([e[1] for e in enc], np.int32)
+        out[key + "_qb"] = np.array([e[2] for e in enc], np.int32)
+        out[key + "_mat"] = np.stack([e[3] for e in enc])
+        out[key + "_sv"] = st.get_statevector()
+        if key == "ghz3":
+            counts = st.get_counts(1024, rng=np.random.default_rng(0))
+            out["ghz3_count_keys"] = np.array(sorted(counts))
+            out["ghz3_count_vals"] = np.array([counts[k] for k in sorted(counts)], np.int64)
+    np.savez_compressed(os.path.join(HERE, "diag_circuits.npz"), **out)
+
+
+def run_xxz():
+    """Low-entanglement case: random product state + XXZ second-order Trotter."""
+    import scipy.linalg as sla
+    n, steps, dt, chi, cutoff, seed = 24, 6, 0.05, 16, 1e-10, 5
+    x = np.array([[0, 1], [1, 0]], complex)
+    y = np.array([[0, -1j], [1j, 0]])
+    z = np.diag([1.0, -1.0]).astype(complex)
+    h = np.kron(x, x) + np.kron(y, y) + 0.5 * np.kron(z, z)
+    half, full = sla.expm(-0.5j * dt * h), sla.expm(-1j * dt * h)
+    rng = np.random.default_rng(seed)
+    th = np.arccos(rng.uniform(-1, 1, n))
+    ph = rng.uniform(0, 2 * np.pi, n)
+    st = mps_core.MPSState(n, chi, cutoff)
+    for i in range(n):
+        st.apply_1q(i, mps_core._gate_1q("u", [th[i], ph[i], 0.0]))
+    seq = []
+    for _ in range(steps):
+        seq += [(i, half) for i in range(1, n - 1, 2)]
+        seq += [(i, full) for i in range(0, n - 1, 2)]
+        seq += [(i, half) for i in range(1, n - 1, 2)]
+    norm_logs = []
+    with Recorder() as rec:
+        for i, g in seq:
+            st._apply_adjacent_2q(i, g)
+            norm_logs.append(st.norm_log)
+    spec, lens = pack_spectra(rec.spectra)
+    bit_rows = np.random.default_rng(seed + 1).integers(0, 2, size=(32, n))
+    np.savez_compressed(os.path.join(HERE, "xxz.npz"), n=n, chi_max=chi, cutoff=cutoff,
+                        theta=th, phi=ph, sites=np.array([i for i, _ in seq], np.int32),
+                        gates=np.stack([g for _, g in seq]), spectra=spec, spec_len=lens,
+                        norm_log=np.array(norm_logs), bits=bit_rows.astype(np.int8),
+                        amps=amplitudes(st, bit_rows), bonds=np.array(st.bond_dims(), np.int32))
+    print("xxz max bond", st.max_bond(), "norm_log", st.norm_log)
+
+
+if __name__ == "__main__":
+    run_gate_tables()
+    run_diag_circuits()
+    run_brick("brick_n16_d10_chi16", 16, 10, 16, 1e-12, 1234, full_sv=True)
+    run_brick("brick_n40_d16_chi32", 40, 16, 32, 1e-10, 77)
+    run_brick("brick_n20_d12_chi64", 20, 12, 64, 1e-10, 4242)
+    run_xxz()

@@ -1,0 +1,88 @@
+"""CPU-side checks: the C-ABI library loads and exports every declared symbol,
+host-only entry points behave, and the host logic around the kernels is right.
+No GPU compute is launched here."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from fpga_mps_simulator_b200 import _lib, gates as G
+from fpga_mps_simulator_b200.mps import validate_pairs
+
+HEADER = os.path.join(ROOT, "include", "mpsb200.h")
+
+
+def _declared():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"MPSB_API\s+[\w\s\*]*?\b(mpsb_\w+)\s*\(", txt)))
+
+
+def test_header_declares_the_binding_exports():
+    assert _declared() == sorted(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    for name in _declared():
+        assert hasattr(lib, name), name
+    assert "sm_100a" in _lib.version()
+
+
+def test_struct_sizes_match_header_layout():
+    # mpsb_chain: 4 pointers, int64, 2 x int32, double
+    assert C.sizeof(_lib.Chain) == 4 * 8 + 8 + 8 + 8
+    assert C.sizeof(_lib.Pair) == 16 and C.sizeof(_lib.SiteOp) == 16
+
+
+def test_workspace_sizes():
+    lib = _lib.load()
+    assert lib.mpsb_update2q_workspace_bytes(10, 65) == 0
+    assert lib.mpsb_update2q_workspace_bytes(-1, 8) == 0
+    w1 = lib.mpsb_update2q_workspace_bytes(1, 64)
+    w2 = lib.mpsb_update2q_workspace_bytes(2, 64)
+    assert w2 - w1 >= 128 * 128 * 16
+
+
+def test_argument_errors_need_no_device():
+    lib = _lib.load()
+    assert lib.mpsb_update2q_batch(None, None, 0, None, 0, 8, 0.0, 0, None, 0, None, None, None, None, None) == 0
+    rc = lib.mpsb_update2q_batch(None, None, -1, None, 0, 8, 0.0, 0, None, 0, None, None, None, None, None)
+    assert rc == -1 and b"npairs" in lib.mpsb_last_error()
+    rc = lib.mpsb_update2q_batch(C.c_void_p(256), C.c_void_p(256), 1, C.c_void_p(256), 0, 99, 0.0, 0,
+                                 C.c_void_p(256), 1 << 30, None, None, None, C.c_void_p(256), None)
+    assert rc == -1 and b"chi_cap" in lib.mpsb_last_error()
+    rc = lib.mpsb_update2q_batch(C.c_void_p(256), C.c_void_p(256), 1, C.c_void_p(256), 7, 8, 0.0, 0,
+                                 C.c_void_p(256), 1 << 30, None, None, None, C.c_void_p(256), None)
+    assert rc == -1 and b"precision" in lib.mpsb_last_error()
+    rc = lib.mpsb_update2q_batch(C.c_void_p(256), C.c_void_p(256), 4, C.c_void_p(256), 0, 8, 0.0, 0,
+                                 C.c_void_p(256), 16, None, None, None, C.c_void_p(256), None)
+    assert rc == -3
+    with pytest.raises(_lib.MPSBError, match="EINVAL"):
+        _lib.check(-1, "probe")
+
+
+def test_validate_pairs():
+    validate_pairs([10], [0, 0, 0], [0, 2, 8])
+    validate_pairs([10, 6], [0, 0, 1, 1], [1, 5, 0, 4])
+    with pytest.raises(ValueError, match="disjoint"):
+        validate_pairs([10], [0, 0], [2, 3])
+    with pytest.raises(ValueError, match="range"):
+        validate_pairs([10], [0], [9])
+    with pytest.raises(ValueError, match="contiguous"):
+        validate_pairs([10, 10], [0, 1, 0], [0, 0, 4])
+    with pytest.raises(ValueError, match="range"):
+        validate_pairs([10], [1], [0])
+
+
+def test_permute_and_route_match_reference_dispatch():
+    g = np.arange(16).reshape(4, 4).astype(complex)
+    p = G.permute_2q(g)
+    # |ab> -> |ba>: row/col 1 <-> 2
+    assert p[1, 2] == g[2, 1] and p[0, 3] == g[0, 3] and p[2, 2] == g[1, 1]
+    route = G.swap_route(5, 1, "cx")
+    assert route == [("swap", [4, 5], None), ("swap", [3, 4], None), ("swap", [2, 3], None),
+                     ("cx", [1, 2], None), ("swap", [2, 3], None), ("swap", [3, 4], None),
+                     ("swap", [4, 5], None)]
