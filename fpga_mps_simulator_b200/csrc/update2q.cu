@@ -26,11 +26,13 @@
 #include "mpsb_common.cuh"
 
 #include <cstdio>
+#include <cstdlib>
 
 namespace mpsb {
 
-constexpr int kUpdThreads = 512;
-constexpr int kUpdWarps = kUpdThreads / 32;
+// CTA size is a template parameter NT (256 or 512 threads): 512 gives one
+// warp per round task at chi = 64 with 128 registers per thread, 256 gives
+// two tasks per warp with up to 255 registers.
 
 struct Upd2Params {
     const mpsb_chain *chains;
@@ -63,79 +65,137 @@ struct CtaScalars {
 
 __host__ __device__ inline size_t upd_smem_bytes(int wmax, int rpad) {
     return 384 + (size_t)3 * wmax * rpad * sizeof(double2) + (size_t)2 * wmax * sizeof(double) +
-           (size_t)4 * wmax * sizeof(double) + (size_t)4 * wmax * sizeof(int);
+           (size_t)4 * wmax * sizeof(double) + (size_t)4 * wmax * sizeof(int) + (size_t)3 * wmax * sizeof(double);
 }
 
 // ------------------------------------------------------------- rotations
-// One complex Jacobi rotation of columns (x, y) given the reduced Gram
-// entries a = |x|^2, b = |y|^2, g = x^H y.  With g = |g| e^{i phi} the pair is
-// the real problem [[a,|g|],[|g|,b]] in the basis (x, e^{-i phi} y); the
-// classical Jacobi angle zeta = (b-a)/(2|g|), t = sgn(zeta)/(|zeta| +
-// sqrt(1+zeta^2)), c = 1/sqrt(1+t^2), s = c t gives
-//   x' = c x - s e^{-i phi} y,  y' = s x + c e^{-i phi} y.
-template <int RPL>
-__device__ __forceinline__ int apply_rotation(double2 (&x)[RPL], double2 (&y)[RPL], double a, double b,
-                                              double gr, double gi, double tol2) {
+// Complex Jacobi rotation of columns (x, y) with a = |x|^2, b = |y|^2 and
+// g = x^H y = |g| e^{i phi}.  In the basis (x, e^{-i phi} y) the pair is the
+// real problem [[a, |g|], [|g|, b]]; the inner rotation (|theta| <= pi/4)
+// that diagonalises it has cos 2theta = |b - a| / sqrt((b - a)^2 + 4|g|^2),
+// sign(theta) = sign(b - a), and acts as
+//   x' = c x - s conj(e) y,   y' = s x + c conj(e) y,
+//   a' = a - t|g|,  b' = b + t|g|   (t = s / c).
+// Everything is built from three reciprocal square roots:
+//   w = 1/sqrt(d^2 + 4 g2), h = cos^2 theta = (1 + |d| w)/2, q = 1/sqrt(h),
+//   c = h q, s/|g| = sign(d) w q, t|g| = sign(d) g2 w q ... (see code).
+// A converged pair (|g|^2 <= tol^2 a b) gets the identity.
+struct Rot {
+    double c, s, er, ei, dl;  // cos, sin, conj phase e = g/|g|, t|g|
+    int go;
+};
+
+__device__ __forceinline__ Rot jacobi_rotation(double a, double b, double gr, double gi, double tol2) {
+    Rot r;
     const double g2 = fma(gr, gr, gi * gi);
-    if (!(g2 > tol2 * (a * b))) return 0;  // converged pair (also rejects NaN)
+    r.go = (g2 > tol2 * (a * b)) && (g2 > 0.0);
+    const double d = b - a;
+    const double w = rsqrt(fma(4.0, g2, d * d));
+    const double h = fma(0.5 * fabs(d), w, 0.5);
+    const double q = rsqrt(h);
     const double rg = rsqrt(g2);
-    const double zeta = 0.5 * (b - a) * rg;
-    double t = 1.0 / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
-    t = copysign(t, zeta);
-    const double c = rsqrt(fma(t, t, 1.0));
-    const double s = c * t;
-    const double er = gr * rg, ei = gi * rg;
-    const double2 zp = make_double2(-s * er, s * ei);  // -s conj(e)
-    const double2 zq = make_double2(c * er, -c * ei);  //  c conj(e)
+    const double sw = copysign(w * q, d);  // s / |g|
+    r.c = r.go ? h * q : 1.0;
+    r.s = r.go ? sw * g2 * rg : 0.0;
+    r.er = r.go ? gr * rg : 1.0;
+    r.ei = r.go ? gi * rg : 0.0;
+    r.dl = r.go ? sw * g2 * q : 0.0;  // t |g|
+    return r;
+}
+
+__device__ __forceinline__ Rot sel_rot(bool first, const Rot &a, const Rot &b) {
+    Rot o;
+    o.c = first ? a.c : b.c;
+    o.s = first ? a.s : b.s;
+    o.er = first ? a.er : b.er;
+    o.ei = first ? a.ei : b.ei;
+    o.dl = first ? a.dl : b.dl;
+    o.go = first ? a.go : b.go;
+    return o;
+}
+
+__device__ __forceinline__ Rot shfl_rot(const Rot &r, int mask) {
+    Rot o;
+    o.c = __shfl_xor_sync(0xffffffffu, r.c, mask);
+    o.s = __shfl_xor_sync(0xffffffffu, r.s, mask);
+    o.er = __shfl_xor_sync(0xffffffffu, r.er, mask);
+    o.ei = __shfl_xor_sync(0xffffffffu, r.ei, mask);
+    o.dl = __shfl_xor_sync(0xffffffffu, r.dl, mask);
+    o.go = __shfl_xor_sync(0xffffffffu, r.go, mask);
+    return o;
+}
+
+// x' = c x - s u, y' = s x + c u with u = conj(e) y.
+template <int RPL>
+__device__ __forceinline__ void apply_rot(double2 (&x)[RPL], double2 (&y)[RPL], const Rot &r) {
 #pragma unroll
-    for (int r = 0; r < RPL; ++r) {
-        const double2 xo = x[r], yo = y[r];
-        x[r] = c_fma(zp, yo, c_scale(xo, c));
-        y[r] = c_fma(zq, yo, c_scale(xo, s));
+    for (int k = 0; k < RPL; ++k) {
+        const double2 xo = x[k], yo = y[k];
+        const double ur = fma(r.er, yo.x, r.ei * yo.y);
+        const double ui = fma(r.er, yo.y, -r.ei * yo.x);
+        x[k] = make_double2(fma(r.c, xo.x, -r.s * ur), fma(r.c, xo.y, -r.s * ui));
+        y[k] = make_double2(fma(r.s, xo.x, r.c * ur), fma(r.s, xo.y, r.c * ui));
     }
-    return 1;
 }
 
 template <int RPL>
-__device__ __forceinline__ void gram_partial(const double2 (&x)[RPL], const double2 (&y)[RPL], double &a,
-                                             double &b, double &gr, double &gi) {
-    a = 0.0; b = 0.0; gr = 0.0; gi = 0.0;
+__device__ __forceinline__ double col_norm2(const double2 (&x)[RPL]) {
+    double a = 0.0;
 #pragma unroll
-    for (int r = 0; r < RPL; ++r) {
-        a = fma(x[r].x, x[r].x, fma(x[r].y, x[r].y, a));
-        b = fma(y[r].x, y[r].x, fma(y[r].y, y[r].y, b));
-        gr = fma(x[r].x, y[r].x, fma(x[r].y, y[r].y, gr));
-        gi = fma(x[r].x, y[r].y, fma(-x[r].y, y[r].x, gi));
-    }
+    for (int k = 0; k < RPL; ++k) a = fma(x[k].x, x[k].x, fma(x[k].y, x[k].y, a));
+    return warp_sum(a);
 }
 
-// Two independent rotations, reductions interleaved for ILP.
+// Norm bookkeeping after a rotation: a' = a - t|g|, b' = b + t|g|.  When the
+// update cancels (a' below 1e-8 of a), the norm is recomputed from the data.
 template <int RPL>
-__device__ __forceinline__ int rotate2(double2 (&x1)[RPL], double2 (&y1)[RPL], double2 (&x2)[RPL],
-                                       double2 (&y2)[RPL], double tol2) {
-    double v[8];
-    gram_partial<RPL>(x1, y1, v[0], v[1], v[2], v[3]);
-    gram_partial<RPL>(x2, y2, v[4], v[5], v[6], v[7]);
+__device__ __forceinline__ void update_norms(const double2 (&x)[RPL], const double2 (&y)[RPL], const Rot &r,
+                                             double &a, double &b) {
+    const double an = a - r.dl, bn = b + r.dl;
+    a = (an < 1e-8 * a) ? col_norm2<RPL>(x) : an;
+    b = (bn < 1e-8 * b) ? col_norm2<RPL>(y) : bn;
+}
+
+// Two independent rotations (x1,y1) and (x2,y2) by one warp.  The inner
+// products are reduced so that lanes 0-15 finish pair 1 and lanes 16-31
+// pair 2; each half computes its rotation once and the halves swap them.
+template <int RPL>
+__device__ __forceinline__ int rotate2(double2 (&x1)[RPL], double2 (&y1)[RPL], double &a1, double &b1,
+                                       double2 (&x2)[RPL], double2 (&y2)[RPL], double &a2, double &b2,
+                                       int lane, double tol2) {
+    double p1r = 0.0, p1i = 0.0, p2r = 0.0, p2i = 0.0;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    for (int k = 0; k < RPL; ++k) {
+        p1r = fma(x1[k].x, y1[k].x, fma(x1[k].y, y1[k].y, p1r));
+        p1i = fma(x1[k].x, y1[k].y, fma(-x1[k].y, y1[k].x, p1i));
+        p2r = fma(x2[k].x, y2[k].x, fma(x2[k].y, y2[k].y, p2r));
+        p2i = fma(x2[k].x, y2[k].y, fma(-x2[k].y, y2[k].x, p2i));
     }
-    int n = apply_rotation<RPL>(x1, y1, v[0], v[1], v[2], v[3], tol2);
-    n += apply_rotation<RPL>(x2, y2, v[4], v[5], v[6], v[7], tol2);
+    const bool lo = lane < 16;
+    double kr = lo ? p1r : p2r, ki = lo ? p1i : p2i;
+    kr += __shfl_xor_sync(0xffffffffu, lo ? p2r : p1r, 16);
+    ki += __shfl_xor_sync(0xffffffffu, lo ? p2i : p1i, 16);
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) {
+        kr += __shfl_xor_sync(0xffffffffu, kr, o);
+        ki += __shfl_xor_sync(0xffffffffu, ki, o);
+    }
+    const Rot mine = jacobi_rotation(lo ? a1 : a2, lo ? b1 : b2, kr, ki, tol2);
+    const Rot other = shfl_rot(mine, 16);
+    int n;
+    {
+        const Rot r1 = sel_rot(lo, mine, other);
+        apply_rot<RPL>(x1, y1, r1);
+        update_norms<RPL>(x1, y1, r1, a1, b1);
+        n = r1.go;
+    }
+    {
+        const Rot r2 = sel_rot(lo, other, mine);
+        apply_rot<RPL>(x2, y2, r2);
+        update_norms<RPL>(x2, y2, r2, a2, b2);
+        n += r2.go;
+    }
     return n;
-}
-
-template <int RPL>
-__device__ __forceinline__ int rotate1(double2 (&x)[RPL], double2 (&y)[RPL], double tol2) {
-    double v[4];
-    gram_partial<RPL>(x, y, v[0], v[1], v[2], v[3]);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
-    }
-    return apply_rotation<RPL>(x, y, v[0], v[1], v[2], v[3], tol2);
 }
 
 template <int RPL>
@@ -149,33 +209,69 @@ __device__ __forceinline__ void store_col(double2 *col, int lane, const double2 
     for (int r = 0; r < RPL; ++r) col[lane + 32 * r] = v[r];
 }
 
-// Warp task: the four cross rotations between duo (p0,p1) and duo (q0,q1).
+// Shared-memory view of the two local slots: column j of slot s at
+// X + (s*wmax + j)*rpad, its squared norm at nrm[s*wmax + j].
+struct Slots {
+    double2 *X;
+    double *nrm;
+    int wmax, rpad;
+    __device__ __forceinline__ double2 *col(int s, int j) const { return X + (size_t)(s * wmax + j) * rpad; }
+    __device__ __forceinline__ double &norm(int s, int j) const { return nrm[s * wmax + j]; }
+};
+
+// Warp task: the four rotations between duo (s0: 2u, 2u+1) and duo (s1: 2v, 2v+1).
 template <int RPL>
-__device__ __forceinline__ int duo_pair(double2 *p0c, double2 *p1c, double2 *q0c, double2 *q1c, int lane,
-                                        double tol2) {
+__device__ __forceinline__ int duo_pair(const Slots &S, int s0, int u, int s1, int v, int lane, double tol2) {
     double2 p0[RPL], p1[RPL], q0[RPL], q1[RPL];
-    load_col<RPL>(p0c, lane, p0);
-    load_col<RPL>(p1c, lane, p1);
-    load_col<RPL>(q0c, lane, q0);
-    load_col<RPL>(q1c, lane, q1);
-    int n = rotate2<RPL>(p0, q0, p1, q1, tol2);
-    n += rotate2<RPL>(p0, q1, p1, q0, tol2);
-    store_col<RPL>(p0c, lane, p0);
-    store_col<RPL>(p1c, lane, p1);
-    store_col<RPL>(q0c, lane, q0);
-    store_col<RPL>(q1c, lane, q1);
+    load_col<RPL>(S.col(s0, 2 * u), lane, p0);
+    load_col<RPL>(S.col(s0, 2 * u + 1), lane, p1);
+    load_col<RPL>(S.col(s1, 2 * v), lane, q0);
+    load_col<RPL>(S.col(s1, 2 * v + 1), lane, q1);
+    double np0 = S.norm(s0, 2 * u), np1 = S.norm(s0, 2 * u + 1);
+    double nq0 = S.norm(s1, 2 * v), nq1 = S.norm(s1, 2 * v + 1);
+    int n = rotate2<RPL>(p0, q0, np0, nq0, p1, q1, np1, nq1, lane, tol2);
+    n += rotate2<RPL>(p0, q1, np0, nq1, p1, q0, np1, nq0, lane, tol2);
+    store_col<RPL>(S.col(s0, 2 * u), lane, p0);
+    store_col<RPL>(S.col(s0, 2 * u + 1), lane, p1);
+    store_col<RPL>(S.col(s1, 2 * v), lane, q0);
+    store_col<RPL>(S.col(s1, 2 * v + 1), lane, q1);
+    if (lane == 0) {
+        S.norm(s0, 2 * u) = np0;
+        S.norm(s0, 2 * u + 1) = np1;
+        S.norm(s1, 2 * v) = nq0;
+        S.norm(s1, 2 * v + 1) = nq1;
+    }
     return n;
 }
 
+// Warp task: the inner pairs of two duos (duo index t covers both slots).
 template <int RPL>
-__device__ __forceinline__ int duo_single(double2 *c0, double2 *c1, int lane, double tol2) {
-    double2 x[RPL], y[RPL];
-    load_col<RPL>(c0, lane, x);
-    load_col<RPL>(c1, lane, y);
-    const int n = rotate1<RPL>(x, y, tol2);
-    store_col<RPL>(c0, lane, x);
-    store_col<RPL>(c1, lane, y);
-    return n;
+__device__ __forceinline__ int duo_inner2(const Slots &S, int nd, int t0, int t1, int lane, double tol2) {
+    const int sa = t0 / nd, da = t0 - sa * nd;
+    const int sb = t1 / nd, db = t1 - sb * nd;
+    double2 x1[RPL], y1[RPL], x2[RPL], y2[RPL];
+    load_col<RPL>(S.col(sa, 2 * da), lane, x1);
+    load_col<RPL>(S.col(sa, 2 * da + 1), lane, y1);
+    load_col<RPL>(S.col(sb, 2 * db), lane, x2);
+    load_col<RPL>(S.col(sb, 2 * db + 1), lane, y2);
+    double a1 = S.norm(sa, 2 * da), b1 = S.norm(sa, 2 * da + 1);
+    double a2 = S.norm(sb, 2 * db), b2 = S.norm(sb, 2 * db + 1);
+    const int n = rotate2<RPL>(x1, y1, a1, b1, x2, y2, a2, b2, lane, tol2);
+    store_col<RPL>(S.col(sa, 2 * da), lane, x1);
+    store_col<RPL>(S.col(sa, 2 * da + 1), lane, y1);
+    if (t1 != t0) {
+        store_col<RPL>(S.col(sb, 2 * db), lane, x2);
+        store_col<RPL>(S.col(sb, 2 * db + 1), lane, y2);
+    }
+    if (lane == 0) {
+        S.norm(sa, 2 * da) = a1;
+        S.norm(sa, 2 * da + 1) = b1;
+        if (t1 != t0) {
+            S.norm(sb, 2 * db) = a2;
+            S.norm(sb, 2 * db + 1) = b2;
+        }
+    }
+    return (t1 != t0) ? n : (n >> 1);
 }
 
 // Element at position k of round r of the circle-method round robin over nd2 items.
@@ -185,15 +281,15 @@ __device__ __forceinline__ int rr_elem(int k, int r, int nd2) {
 
 // One block-step of a sweep inside a CTA: (optionally) all pairs inside each
 // of the two slots, then all pairs between slot 0 and slot 1.
-template <int RPL>
-__device__ void step_rounds(double2 *X, int w, int wmax, int rpad, bool internal, int warp, int lane,
-                            double tol2, int &cnt) {
+template <int RPL, int NT>
+__device__ void step_rounds(const Slots &S, int w, bool internal, int warp, int lane, double tol2, int &cnt) {
+    constexpr int kUpdWarps = NT / 32;
     const int nd = w >> 1;
-    auto col = [&](int slot, int j) { return X + (size_t)(slot * wmax + j) * rpad; };
     if (internal) {
-        for (int t = warp; t < 2 * nd; t += kUpdWarps) {
-            const int slot = t / nd, d = t - slot * nd;
-            cnt += duo_single<RPL>(col(slot, 2 * d), col(slot, 2 * d + 1), lane, tol2);
+        // inner pairs of all 2*nd duos, two duos per warp (an odd last one is paired with itself)
+        for (int t = 2 * warp; t < 2 * nd; t += 2 * kUpdWarps) {
+            const int t1 = (t + 1 < 2 * nd) ? t + 1 : t;
+            cnt += duo_inner2<RPL>(S, nd, t, t1, lane, tol2);
         }
         __syncthreads();
         const int nd2 = nd + (nd & 1);
@@ -202,9 +298,7 @@ __device__ void step_rounds(double2 *X, int w, int wmax, int rpad, bool internal
             for (int t = warp; t < 2 * half; t += kUpdWarps) {
                 const int slot = t / half, k = t - slot * half;
                 const int u = rr_elem(k, r, nd2), v = rr_elem(nd2 - 1 - k, r, nd2);
-                if (u < nd && v < nd)
-                    cnt += duo_pair<RPL>(col(slot, 2 * u), col(slot, 2 * u + 1), col(slot, 2 * v),
-                                         col(slot, 2 * v + 1), lane, tol2);
+                if (u < nd && v < nd) cnt += duo_pair<RPL>(S, slot, u, slot, v, lane, tol2);
             }
             __syncthreads();
         }
@@ -213,34 +307,56 @@ __device__ void step_rounds(double2 *X, int w, int wmax, int rpad, bool internal
         for (int t = warp; t < nd; t += kUpdWarps) {
             int v = t + r;
             if (v >= nd) v -= nd;
-            cnt += duo_pair<RPL>(col(0, 2 * t), col(0, 2 * t + 1), col(1, 2 * v), col(1, 2 * v + 1), lane,
-                                 tol2);
+            cnt += duo_pair<RPL>(S, 0, t, 1, v, lane, tol2);
         }
         __syncthreads();
     }
 }
 
-// Swap one slot with the partner CTA.  Pattern A (parity 0): CTA0.slot1 <->
-// CTA1.slot0; pattern B (parity 1): CTA0.slot1 <-> CTA1.slot1.  Alternating
-// A, B, A, ... after every step visits all six block pairs once per sweep.
-// Each CTA stores its outgoing block into the partner's staging area through
-// distributed shared memory, then copies its own staging area into the slot.
-__device__ void exchange_slots(cg::cluster_group &cluster, double2 *X, double2 *stage, int crank, int parity,
-                               int w, int wmax, int rpad, int tid) {
-    const int my_slot = (crank == 0) ? 1 : parity;
-    const int n_el = w * rpad;
-    double2 *mine = X + (size_t)my_slot * wmax * rpad;
-    double2 *their_stage = cluster.map_shared_rank(stage, crank ^ 1);
-    cluster.sync();  // partner finished its rounds and its previous staging copy
-    for (int e = tid; e < n_el; e += kUpdThreads) their_stage[e] = mine[e];
-    cluster.sync();  // both staging areas filled
-    for (int e = tid; e < n_el; e += kUpdThreads) mine[e] = stage[e];
+// Exact squared norms of the 2w local columns (start of every sweep).
+template <int RPL, int NT>
+__device__ void recompute_norms(const Slots &S, int w, int warp, int lane) {
+    constexpr int kUpdWarps = NT / 32;
+    for (int j = warp; j < 2 * w; j += kUpdWarps) {
+        const int slot = j >= w, jj = j - slot * w;
+        double2 v[RPL];
+        load_col<RPL>(S.col(slot, jj), lane, v);
+        const double a = col_norm2<RPL>(v);
+        if (lane == 0) S.norm(slot, jj) = a;
+    }
     __syncthreads();
 }
 
-template <int RPL>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kUpdThreads, 1)
+// Swap one slot (columns and norms) with the partner CTA.  Pattern A
+// (parity 0): CTA0.slot1 <-> CTA1.slot0; pattern B (parity 1): CTA0.slot1 <->
+// CTA1.slot1.  Alternating A, B, A, ... after every step visits all six block
+// pairs once per sweep.  Each CTA stores its outgoing block into the
+// partner's staging area through distributed shared memory, then copies its
+// own staging area into the slot.
+template <int NT>
+__device__ void exchange_slots(cg::cluster_group &cluster, const Slots &S, double2 *stage, double *stage_nrm,
+                               int crank, int parity, int w, int tid) {
+    constexpr int kUpdThreads = NT;
+    const int my_slot = (crank == 0) ? 1 : parity;
+    const int n_el = w * S.rpad;
+    double2 *mine = S.col(my_slot, 0);
+    double *mine_nrm = &S.norm(my_slot, 0);
+    double2 *their_stage = cluster.map_shared_rank(stage, crank ^ 1);
+    double *their_nrm = cluster.map_shared_rank(stage_nrm, crank ^ 1);
+    cluster.sync();  // partner finished its rounds and its previous staging copy
+    for (int e = tid; e < n_el; e += kUpdThreads) their_stage[e] = mine[e];
+    if (tid < w) their_nrm[tid] = mine_nrm[tid];
+    cluster.sync();  // both staging areas filled
+    for (int e = tid; e < n_el; e += kUpdThreads) mine[e] = stage[e];
+    if (tid < w) mine_nrm[tid] = stage_nrm[tid];
+    __syncthreads();
+}
+
+template <int RPL, int NT>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
     update2q_fp64_kernel(const Upd2Params p) {
+    constexpr int kUpdThreads = NT;
+    constexpr int kUpdWarps = NT / 32;
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank();
     const int pi = (int)(blockIdx.x >> 1);
@@ -255,6 +371,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kUpdThreads, 1)
     double *Ssorted = sig2 + 2 * wmax;
     int *rank = reinterpret_cast<int *>(Ssorted + 4 * wmax);
     int *klist = rank + 2 * wmax;
+    double *nrm = reinterpret_cast<double *>(klist + 2 * wmax);
+    double *stage_nrm = nrm + 2 * wmax;
+    const Slots S{X, nrm, wmax, rpad};
 
     const mpsb_pair pr = p.pairs[pi];
     const mpsb_chain ch = p.chains[pr.chain];
@@ -362,12 +481,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kUpdThreads, 1)
     for (int sweep = 0; sweep < p.max_sweeps; ++sweep) {
         const int sb = sweep & 1;
         if (tid == 0) sc->nrot[sb] = 0;
-        __syncthreads();
+        recompute_norms<RPL, NT>(S, w, warp, lane);
         int cnt = 0;
         for (int step = 0; step < 3; ++step) {
-            step_rounds<RPL>(X, w, wmax, rpad, step == 0, warp, lane, p.tol2, cnt);
+            step_rounds<RPL, NT>(S, w, step == 0, warp, lane, p.tol2, cnt);
             if (step == 2 && lane == 0 && cnt) atomicAdd(&sc->nrot[sb], cnt);
-            exchange_slots(cluster, X, stage, crank, parity, w, wmax, rpad, tid);
+            exchange_slots<NT>(cluster, S, stage, stage_nrm, crank, parity, w, tid);
             parity ^= 1;
         }
         const int remote = *cluster.map_shared_rank(&sc->nrot[sb], crank ^ 1);
@@ -481,9 +600,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kUpdThreads, 1)
     // other side: Y[rho, col] = sum_r conj(x_j[r]) X0[r, col]
     {
         const double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
+        constexpr int kGroups = NT / 128;
         const int col = tid & 127, grp = tid >> 7;
         if (col < C) {
-            for (int base = grp * 8; base < nk; base += 32) {
+            for (int base = grp * 8; base < nk; base += 8 * kGroups) {
                 const int nb = min(8, nk - base);
                 const double2 *cpk[8];
                 double2 acc[8];
@@ -545,17 +665,29 @@ size_t upd_workspace_bytes(int npairs, int chi_cap) {
     return align256((size_t)npairs * sizeof(PairRec)) + (size_t)npairs * x0_stride * sizeof(double2);
 }
 
-template <int RPL>
+template <int RPL, int NT>
 static int launch_rpl(const Upd2Params &p, size_t smem, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
-        if (cudaFuncSetAttribute(update2q_fp64_kernel<RPL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(update2q_fp64_kernel<RPL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return check_launch("cudaFuncSetAttribute(update2q)");
         configured = true;
     }
-    update2q_fp64_kernel<RPL><<<2 * p.npairs, kUpdThreads, smem, s>>>(p);
+    update2q_fp64_kernel<RPL, NT><<<2 * p.npairs, NT, smem, s>>>(p);
     return check_launch("update2q_fp64_kernel");
+}
+
+// CTA size per rows-per-lane class; MPSB_UPD_THREADS=256|512 overrides (tuning).
+static int upd_threads(int rpl) {
+    static int forced = -1;
+    if (forced < 0) {
+        const char *e = getenv("MPSB_UPD_THREADS");
+        forced = e ? atoi(e) : 0;
+    }
+    if (forced == 256 || forced == 512) return forced;
+    (void)rpl;
+    return 256;
 }
 
 int launch_update2q(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const double2 *gates,
@@ -582,11 +714,12 @@ int launch_update2q(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs
     p.max_sweeps = max_sweeps;
     const size_t smem = upd_smem_bytes(p.wmax, p.rpad);
     int rc;
+    const bool big = upd_threads(rpl) == 512;
     switch (rpl) {
-        case 1: rc = launch_rpl<1>(p, smem, stream); break;
-        case 2: rc = launch_rpl<2>(p, smem, stream); break;
-        case 3: rc = launch_rpl<3>(p, smem, stream); break;
-        default: rc = launch_rpl<4>(p, smem, stream); break;
+        case 1: rc = big ? launch_rpl<1, 512>(p, smem, stream) : launch_rpl<1, 256>(p, smem, stream); break;
+        case 2: rc = big ? launch_rpl<2, 512>(p, smem, stream) : launch_rpl<2, 256>(p, smem, stream); break;
+        case 3: rc = big ? launch_rpl<3, 512>(p, smem, stream) : launch_rpl<3, 256>(p, smem, stream); break;
+        default: rc = big ? launch_rpl<4, 512>(p, smem, stream) : launch_rpl<4, 256>(p, smem, stream); break;
     }
     if (rc != MPSB_OK) return rc;
     fold_norm_log_kernel<<<(npairs + 127) / 128, 128, 0, stream>>>(chains, pairs, npairs, p.rec);

@@ -179,7 +179,7 @@ class OracleMPS:
         e, acc = envs[0], 0.0
         for k in range(self.n):
             a = self.sites[k]
-            e = np.einsum("xy,xsc,ysd->cd", e, a.conj(), a)
+            e = np.einsum("xsc,xsd->cd", a.conj(), np.einsum("xy,ysd->xsd", e, a))
             tr = float(np.real(np.trace(e)))
             if tr > 0:
                 e = e / tr
@@ -194,7 +194,7 @@ class OracleMPS:
         e, acc = envs[self.n], 0.0
         for k in range(self.n - 1, -1, -1):
             a = self.sites[k]
-            e = np.einsum("csx,dsy,xy->cd", a.conj(), a, e)
+            e = np.einsum("csx,dsx->cd", a.conj(), np.einsum("dsy,xy->dsx", a, e))
             tr = float(np.real(np.trace(e)))
             if tr > 0:
                 e = e / tr
@@ -208,25 +208,29 @@ class OracleMPS:
         L, lg = self._transfer_left()
         return float(np.real(L[self.n][0, 0])) * math.exp(lg[self.n] + 2.0 * self.norm_log)
 
-    def expect_local(self, ops: Dict[int, np.ndarray]) -> float:
+    def expect_local(self, ops: Dict[int, np.ndarray], envs=None) -> float:
         """Normalised <psi| prod_k O_k |psi> / <psi|psi> for operators on a contiguous site range."""
         sites = sorted(ops)
         lo, hi = sites[0], sites[-1]
-        L, _ = self._transfer_left()
-        R, _ = self._transfer_right()
+        L, R = envs if envs is not None else (self._transfer_left()[0], self._transfer_right()[0])
         num, den = L[lo], L[lo]
         for k in range(lo, hi + 1):
             a = self.sites[k]
             op = ops.get(k, np.eye(2, dtype=np.complex128))
-            num = np.einsum("xy,xsc,st,ytd->cd", num, a.conj(), op, a)
-            den = np.einsum("xy,xsc,ysd->cd", den, a.conj(), a)
+            num = np.einsum("xsc,xsd->cd", a.conj(), np.einsum("st,xy,ytd->xsd", op, num, a, optimize=True))
+            den = np.einsum("xsc,xsd->cd", a.conj(), np.einsum("xy,ysd->xsd", den, a))
         val = np.einsum("cd,cd->", num, R[hi + 1])
         nrm = np.einsum("cd,cd->", den, R[hi + 1])
         return float(np.real(val / nrm))
 
+    def environments(self):
+        """(left, right) trace-normalised environments, reusable across expect_local calls."""
+        return self._transfer_left()[0], self._transfer_right()[0]
+
     def expect_z_all(self) -> np.ndarray:
         z = np.diag([1.0, -1.0]).astype(np.complex128)
-        return np.array([self.expect_local({k: z}) for k in range(self.n)])
+        envs = self.environments()
+        return np.array([self.expect_local({k: z}, envs) for k in range(self.n)])
 
     # -- sampling (mps_core.py:354-429) -------------------------------------
     def right_environments(self) -> List[np.ndarray]:
@@ -234,7 +238,7 @@ class OracleMPS:
         out[self.n] = np.ones((1, 1), np.complex128)
         for k in range(self.n - 1, -1, -1):
             a = self.sites[k]
-            e = np.einsum("isb,bc,jsc->ij", a, out[k + 1], a.conj())
+            e = np.einsum("isb,jsb->ij", np.einsum("isc,bc->isb", a, out[k + 1]), a.conj())
             tr = float(np.real(np.trace(e)))
             if tr > 1e-300:
                 e = e / tr

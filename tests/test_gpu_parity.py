@@ -160,7 +160,8 @@ def test_local_expectations_against_oracle():
     terms = [(k, Z, None) for k in range(n)] + [(k, X, None) for k in range(n)] + \
             [(k, Z, Z) for k in range(n - 1)] + [(k, X, Y) for k in range(n - 1)]
     got = st.expect_terms(terms)
-    want = [ref.expect_local({k: a} if b is None else {k: a, k + 1: b}) for k, a, b in terms]
+    envs = ref.environments()
+    want = [ref.expect_local({k: a} if b is None else {k: a, k + 1: b}, envs) for k, a, b in terms]
     np.testing.assert_allclose(got, want, rtol=0, atol=1e-10)
     # Pauli-string form (Qiskit order: leftmost char = qubit n-1)
     s = ["I"] * n
