@@ -123,6 +123,25 @@ MPSB_API int mpsb_update2q_batch(const mpsb_chain *chains, const mpsb_pair *pair
                         double *spectra, int32_t *kept, double *trunc, int32_t *status,
                         mpsb_stream_t stream);
 
+/* Allocation-free form of mpsb_update2q_batch.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory -- a host that
+ * hands the library only buffers registered up front, or a loop in which a
+ * cudaMalloc would synchronise the device -- this entry takes the same inputs
+ * and outputs but no workspace: its scratch is a fixed device array of
+ * MPSB_NOALLOC_SCRATCH_BYTES (16 MiB: 63 pairs at chi_cap = 64, more at smaller
+ * chi_cap) that every GPU loading the library holds until exit.  Batches that
+ * need more scratch are rejected with MPSB_EWORKSPACE before any launch.  The
+ * first call on a device looks up the array's device address (set-up), so
+ * make that first call before any stream capture.  All calls share the
+ * array: calls whose kernels overlap on the GPU race, serialise them on one
+ * stream.  It allocates nothing (no cudaMalloc, no cudaFree). */
+#define MPSB_NOALLOC_SCRATCH_BYTES (16u << 20)
+MPSB_API int mpsb_update2q_batch_noalloc(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+                                         const mpsb_c128 *gates, int precision, int chi_cap,
+                                         double tol, int max_sweeps,
+                                         double *spectra, int32_t *kept, double *trunc, int32_t *status,
+                                         mpsb_stream_t stream);
+
 /* Batched single-site gates, A'[l,s',r] = sum_s G[s',s] A[l,s,r], in place
  * (mps_core.py:267-273; fpga_mps_simulator.cpp:232-276 apply_1q_gate).
  * Ops of one call must touch distinct sites. */
