@@ -30,9 +30,9 @@
 
 namespace mpsb {
 
-// CTA size is a template parameter NT (256 or 512 threads): 512 gives one
-// warp per round task at chi = 64 with 128 registers per thread, 256 gives
-// two tasks per warp with up to 255 registers.
+// 256 threads per CTA: eight warps, one column-quad task per warp and round
+// at chi = 64 (a slot holds up to eight quads), up to 255 registers each.
+constexpr int kUpdThreads = 256;
 
 struct Upd2Params {
     const mpsb_chain *chains;
@@ -58,11 +58,13 @@ struct CtaScalars {
     int nonfinite;
     int keep;
     int nk;
-    int pad0;
+    int timeout;
     double div;
     double2 gate[16];
+    int stamp[16];  // per column quad (slot * 8 + quad): rounds completed in the current step
 };
 
+// Dynamic shared memory: scalars, slots, staging block, spectrum/rank arrays, norms.
 __host__ __device__ inline size_t upd_smem_bytes(int wmax, int rpad) {
     return 384 + (size_t)3 * wmax * rpad * sizeof(double2) + (size_t)2 * wmax * sizeof(double) +
            (size_t)4 * wmax * sizeof(double) + (size_t)4 * wmax * sizeof(int) + (size_t)3 * wmax * sizeof(double);
@@ -103,28 +105,6 @@ __device__ __forceinline__ Rot jacobi_rotation(double a, double b, double gr, do
     return r;
 }
 
-__device__ __forceinline__ Rot sel_rot(bool first, const Rot &a, const Rot &b) {
-    Rot o;
-    o.c = first ? a.c : b.c;
-    o.s = first ? a.s : b.s;
-    o.er = first ? a.er : b.er;
-    o.ei = first ? a.ei : b.ei;
-    o.dl = first ? a.dl : b.dl;
-    o.go = first ? a.go : b.go;
-    return o;
-}
-
-__device__ __forceinline__ Rot shfl_rot(const Rot &r, int mask) {
-    Rot o;
-    o.c = __shfl_xor_sync(0xffffffffu, r.c, mask);
-    o.s = __shfl_xor_sync(0xffffffffu, r.s, mask);
-    o.er = __shfl_xor_sync(0xffffffffu, r.er, mask);
-    o.ei = __shfl_xor_sync(0xffffffffu, r.ei, mask);
-    o.dl = __shfl_xor_sync(0xffffffffu, r.dl, mask);
-    o.go = __shfl_xor_sync(0xffffffffu, r.go, mask);
-    return o;
-}
-
 // x' = c x - s u, y' = s x + c u with u = conj(e) y.
 template <int RPL>
 __device__ __forceinline__ void apply_rot(double2 (&x)[RPL], double2 (&y)[RPL], const Rot &r) {
@@ -149,53 +129,15 @@ __device__ __forceinline__ double col_norm2(const double2 (&x)[RPL]) {
 // Norm bookkeeping after a rotation: a' = a - t|g|, b' = b + t|g|.  When the
 // update cancels (a' below 1e-8 of a), the norm is recomputed from the data.
 template <int RPL>
-__device__ __forceinline__ void update_norms(const double2 (&x)[RPL], const double2 (&y)[RPL], const Rot &r,
-                                             double &a, double &b) {
-    const double an = a - r.dl, bn = b + r.dl;
-    a = (an < 1e-8 * a) ? col_norm2<RPL>(x) : an;
-    b = (bn < 1e-8 * b) ? col_norm2<RPL>(y) : bn;
-}
-
-// Two independent rotations (x1,y1) and (x2,y2) by one warp.  The inner
-// products are reduced so that lanes 0-15 finish pair 1 and lanes 16-31
-// pair 2; each half computes its rotation once and the halves swap them.
-template <int RPL>
-__device__ __forceinline__ int rotate2(double2 (&x1)[RPL], double2 (&y1)[RPL], double &a1, double &b1,
-                                       double2 (&x2)[RPL], double2 (&y2)[RPL], double &a2, double &b2,
-                                       int lane, double tol2) {
-    double p1r = 0.0, p1i = 0.0, p2r = 0.0, p2i = 0.0;
+__device__ __forceinline__ void inner_partial(const double2 (&x)[RPL], const double2 (&y)[RPL], double &re,
+                                              double &im) {
+    re = 0.0;
+    im = 0.0;
 #pragma unroll
     for (int k = 0; k < RPL; ++k) {
-        p1r = fma(x1[k].x, y1[k].x, fma(x1[k].y, y1[k].y, p1r));
-        p1i = fma(x1[k].x, y1[k].y, fma(-x1[k].y, y1[k].x, p1i));
-        p2r = fma(x2[k].x, y2[k].x, fma(x2[k].y, y2[k].y, p2r));
-        p2i = fma(x2[k].x, y2[k].y, fma(-x2[k].y, y2[k].x, p2i));
+        re = fma(x[k].x, y[k].x, fma(x[k].y, y[k].y, re));
+        im = fma(x[k].x, y[k].y, fma(-x[k].y, y[k].x, im));
     }
-    const bool lo = lane < 16;
-    double kr = lo ? p1r : p2r, ki = lo ? p1i : p2i;
-    kr += __shfl_xor_sync(0xffffffffu, lo ? p2r : p1r, 16);
-    ki += __shfl_xor_sync(0xffffffffu, lo ? p2i : p1i, 16);
-#pragma unroll
-    for (int o = 8; o > 0; o >>= 1) {
-        kr += __shfl_xor_sync(0xffffffffu, kr, o);
-        ki += __shfl_xor_sync(0xffffffffu, ki, o);
-    }
-    const Rot mine = jacobi_rotation(lo ? a1 : a2, lo ? b1 : b2, kr, ki, tol2);
-    const Rot other = shfl_rot(mine, 16);
-    int n;
-    {
-        const Rot r1 = sel_rot(lo, mine, other);
-        apply_rot<RPL>(x1, y1, r1);
-        update_norms<RPL>(x1, y1, r1, a1, b1);
-        n = r1.go;
-    }
-    {
-        const Rot r2 = sel_rot(lo, other, mine);
-        apply_rot<RPL>(x2, y2, r2);
-        update_norms<RPL>(x2, y2, r2, a2, b2);
-        n += r2.go;
-    }
-    return n;
 }
 
 template <int RPL>
@@ -219,59 +161,154 @@ struct Slots {
     __device__ __forceinline__ double &norm(int s, int j) const { return nrm[s * wmax + j]; }
 };
 
-// Warp task: the four rotations between duo (s0: 2u, 2u+1) and duo (s1: 2v, 2v+1).
+// ----------------------------------------------------------- warp tasks
+__device__ __forceinline__ Rot shfl_rot_from(const Rot &r, int src) {
+    Rot o;
+    o.c = __shfl_sync(0xffffffffu, r.c, src);
+    o.s = __shfl_sync(0xffffffffu, r.s, src);
+    o.er = __shfl_sync(0xffffffffu, r.er, src);
+    o.ei = __shfl_sync(0xffffffffu, r.ei, src);
+    o.dl = __shfl_sync(0xffffffffu, r.dl, src);
+    o.go = __shfl_sync(0xffffffffu, r.go, src);
+    return o;
+}
+
+// Norm bookkeeping after a rotation: a' = a - t|g|, b' = b + t|g|.  When the
+// update cancels (a' below 1e-8 of a), the norm is recomputed from the data
+// (the warp holds whole columns, the test is uniform across the warp).
 template <int RPL>
-__device__ __forceinline__ int duo_pair(const Slots &S, int s0, int u, int s1, int v, int lane, double tol2) {
-    double2 p0[RPL], p1[RPL], q0[RPL], q1[RPL];
-    load_col<RPL>(S.col(s0, 2 * u), lane, p0);
-    load_col<RPL>(S.col(s0, 2 * u + 1), lane, p1);
-    load_col<RPL>(S.col(s1, 2 * v), lane, q0);
-    load_col<RPL>(S.col(s1, 2 * v + 1), lane, q1);
-    double np0 = S.norm(s0, 2 * u), np1 = S.norm(s0, 2 * u + 1);
-    double nq0 = S.norm(s1, 2 * v), nq1 = S.norm(s1, 2 * v + 1);
-    int n = rotate2<RPL>(p0, q0, np0, nq0, p1, q1, np1, nq1, lane, tol2);
-    n += rotate2<RPL>(p0, q1, np0, nq1, p1, q0, np1, nq0, lane, tol2);
-    store_col<RPL>(S.col(s0, 2 * u), lane, p0);
-    store_col<RPL>(S.col(s0, 2 * u + 1), lane, p1);
-    store_col<RPL>(S.col(s1, 2 * v), lane, q0);
-    store_col<RPL>(S.col(s1, 2 * v + 1), lane, q1);
-    if (lane == 0) {
-        S.norm(s0, 2 * u) = np0;
-        S.norm(s0, 2 * u + 1) = np1;
-        S.norm(s1, 2 * v) = nq0;
-        S.norm(s1, 2 * v + 1) = nq1;
+__device__ __forceinline__ void update_norms(const double2 (&x)[RPL], const double2 (&y)[RPL], const Rot &r,
+                                             double &a, double &b) {
+    const double an = a - r.dl, bn = b + r.dl;
+    a = (an < 1e-8 * a) ? col_norm2<RPL>(x) : an;
+    b = (bn < 1e-8 * b) ? col_norm2<RPL>(y) : bn;
+}
+
+template <int RPL>
+__device__ __forceinline__ int apply_one(double2 (&x)[RPL], double2 (&y)[RPL], double &a, double &b,
+                                         const Rot &mine, int src) {
+    const Rot r = shfl_rot_from(mine, src);
+    apply_rot<RPL>(x, y, r);
+    update_norms<RPL>(x, y, r, a, b);
+    return r.go;
+}
+
+// Four independent rotations (x_j, y_j), j = 0..3, by one warp.  The inner
+// products x_j^H y_j are reduced so that the 8-lane group j = lane >> 3 ends
+// with pair j's sum (two halving exchanges, then a 3-level butterfly inside
+// the group); each group computes its rotation once and the four rotations
+// are broadcast from lanes 0, 8, 16, 24.
+template <int RPL>
+__device__ __forceinline__ int rotate4(double2 (&x0)[RPL], double2 (&y0)[RPL], double &a0, double &b0,
+                                       double2 (&x1)[RPL], double2 (&y1)[RPL], double &a1, double &b1,
+                                       double2 (&x2)[RPL], double2 (&y2)[RPL], double &a2, double &b2,
+                                       double2 (&x3)[RPL], double2 (&y3)[RPL], double &a3, double &b3, int lane,
+                                       double tol2) {
+    double r0, i0, r1, i1, r2, i2, r3, i3;
+    inner_partial<RPL>(x0, y0, r0, i0);
+    inner_partial<RPL>(x1, y1, r1, i1);
+    inner_partial<RPL>(x2, y2, r2, i2);
+    inner_partial<RPL>(x3, y3, r3, i3);
+    const bool h = (lane & 16) != 0;  // keeps pairs {2,3} instead of {0,1}
+    double k0r = h ? r2 : r0, k0i = h ? i2 : i0, k1r = h ? r3 : r1, k1i = h ? i3 : i1;
+    k0r += __shfl_xor_sync(0xffffffffu, h ? r0 : r2, 16);
+    k0i += __shfl_xor_sync(0xffffffffu, h ? i0 : i2, 16);
+    k1r += __shfl_xor_sync(0xffffffffu, h ? r1 : r3, 16);
+    k1i += __shfl_xor_sync(0xffffffffu, h ? i1 : i3, 16);
+    const bool g = (lane & 8) != 0;  // keeps the second of the two
+    double kr = g ? k1r : k0r, ki = g ? k1i : k0i;
+    kr += __shfl_xor_sync(0xffffffffu, g ? k0r : k1r, 8);
+    ki += __shfl_xor_sync(0xffffffffu, g ? k0i : k1i, 8);
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+        kr += __shfl_xor_sync(0xffffffffu, kr, o);
+        ki += __shfl_xor_sync(0xffffffffu, ki, o);
     }
+    const int j = lane >> 3;
+    const double a = j == 0 ? a0 : (j == 1 ? a1 : (j == 2 ? a2 : a3));
+    const double b = j == 0 ? b0 : (j == 1 ? b1 : (j == 2 ? b2 : b3));
+    const Rot mine = jacobi_rotation(a, b, kr, ki, tol2);
+    int n = apply_one<RPL>(x0, y0, a0, b0, mine, 0);
+    n += apply_one<RPL>(x1, y1, a1, b1, mine, 8);
+    n += apply_one<RPL>(x2, y2, a2, b2, mine, 16);
+    n += apply_one<RPL>(x3, y3, a3, b3, mine, 24);
     return n;
 }
 
-// Warp task: the inner pairs of two duos (duo index t covers both slots).
+// Column quads in registers: quad q of slot s is columns 4q..4q+3.
 template <int RPL>
-__device__ __forceinline__ int duo_inner2(const Slots &S, int nd, int t0, int t1, int lane, double tol2) {
-    const int sa = t0 / nd, da = t0 - sa * nd;
-    const int sb = t1 / nd, db = t1 - sb * nd;
-    double2 x1[RPL], y1[RPL], x2[RPL], y2[RPL];
-    load_col<RPL>(S.col(sa, 2 * da), lane, x1);
-    load_col<RPL>(S.col(sa, 2 * da + 1), lane, y1);
-    load_col<RPL>(S.col(sb, 2 * db), lane, x2);
-    load_col<RPL>(S.col(sb, 2 * db + 1), lane, y2);
-    double a1 = S.norm(sa, 2 * da), b1 = S.norm(sa, 2 * da + 1);
-    double a2 = S.norm(sb, 2 * db), b2 = S.norm(sb, 2 * db + 1);
-    const int n = rotate2<RPL>(x1, y1, a1, b1, x2, y2, a2, b2, lane, tol2);
-    store_col<RPL>(S.col(sa, 2 * da), lane, x1);
-    store_col<RPL>(S.col(sa, 2 * da + 1), lane, y1);
-    if (t1 != t0) {
-        store_col<RPL>(S.col(sb, 2 * db), lane, x2);
-        store_col<RPL>(S.col(sb, 2 * db + 1), lane, y2);
+__device__ __forceinline__ void load_quad(const Slots &S, int s, int q, int lane, double2 (&X)[4][RPL],
+                                          double (&nr)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        load_col<RPL>(S.col(s, 4 * q + k), lane, X[k]);
+        nr[k] = S.norm(s, 4 * q + k);
     }
+}
+template <int RPL>
+__device__ __forceinline__ void store_quad(const Slots &S, int s, int q, int lane, const double2 (&X)[4][RPL],
+                                           const double (&nr)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) store_col<RPL>(S.col(s, 4 * q + k), lane, X[k]);
     if (lane == 0) {
-        S.norm(sa, 2 * da) = a1;
-        S.norm(sa, 2 * da + 1) = b1;
-        if (t1 != t0) {
-            S.norm(sb, 2 * db) = a2;
-            S.norm(sb, 2 * db + 1) = b2;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) S.norm(s, 4 * q + k) = nr[k];
+    }
+}
+
+// The sixteen rotations between quads P and Q, four disjoint ones per phase
+// (phase k pairs P_i with Q_{(i+k) mod 4}).
+template <int RPL>
+__device__ __forceinline__ int quad_cross(double2 (&P)[4][RPL], double (&p)[4], double2 (&Q)[4][RPL], double (&q)[4],
+                                          int lane, double tol2) {
+    int n = rotate4<RPL>(P[0], Q[0], p[0], q[0], P[1], Q[1], p[1], q[1], P[2], Q[2], p[2], q[2], P[3], Q[3], p[3],
+                         q[3], lane, tol2);
+    n += rotate4<RPL>(P[0], Q[1], p[0], q[1], P[1], Q[2], p[1], q[2], P[2], Q[3], p[2], q[3], P[3], Q[0], p[3], q[0],
+                      lane, tol2);
+    n += rotate4<RPL>(P[0], Q[2], p[0], q[2], P[1], Q[3], p[1], q[3], P[2], Q[0], p[2], q[0], P[3], Q[1], p[3], q[1],
+                      lane, tol2);
+    n += rotate4<RPL>(P[0], Q[3], p[0], q[3], P[1], Q[0], p[1], q[0], P[2], Q[1], p[2], q[1], P[3], Q[2], p[3], q[2],
+                      lane, tol2);
+    return n;
+}
+
+// The six inner pairs of quad A and of quad B, three phases of four rotations.
+template <int RPL>
+__device__ __forceinline__ int quad_inner2(double2 (&A)[4][RPL], double (&a)[4], double2 (&B)[4][RPL],
+                                           double (&b)[4], int lane, double tol2) {
+    int n = rotate4<RPL>(A[0], A[1], a[0], a[1], A[2], A[3], a[2], a[3], B[0], B[1], b[0], b[1], B[2], B[3], b[2],
+                         b[3], lane, tol2);
+    n += rotate4<RPL>(A[0], A[2], a[0], a[2], A[1], A[3], a[1], a[3], B[0], B[2], b[0], b[2], B[1], B[3], b[1], b[3],
+                      lane, tol2);
+    n += rotate4<RPL>(A[0], A[3], a[0], a[3], A[1], A[2], a[1], a[2], B[0], B[3], b[0], b[3], B[1], B[2], b[1], b[2],
+                      lane, tol2);
+    return n;
+}
+
+// Dataflow between the warps of a CTA.  Every column quad carries a stamp =
+// the number of rounds of the current step it has been through; a warp
+// starts a round-r task once both of its quads reach stamp r, so warps drift
+// apart instead of meeting at a barrier every round (their reduction and
+// angle latencies then overlap other warps' FP64 work).  The wait is bounded:
+// after 2^26 polls it records a timeout (status bit MPSB_ST_TIMEOUT) and
+// goes on, so a scheduling fault can never hang the GPU.
+__device__ __forceinline__ void wait_stamp(const int *st, int target, int lane, int &tmo) {
+    if (lane == 0) {
+        unsigned polls = 0;
+        while (*reinterpret_cast<const volatile int *>(st) < target) {
+            if (++polls > (1u << 26)) {
+                tmo = 1;
+                break;
+            }
         }
     }
-    return (t1 != t0) ? n : (n >> 1);
+    __syncwarp();
+    __threadfence_block();
+}
+__device__ __forceinline__ void set_stamp(int *st, int value, int lane) {
+    __syncwarp();
+    __threadfence_block();
+    if (lane == 0) *reinterpret_cast<volatile int *>(st) = value;
 }
 
 // Element at position k of round r of the circle-method round robin over nd2 items.
@@ -279,41 +316,83 @@ __device__ __forceinline__ int rr_elem(int k, int r, int nd2) {
     return k == 0 ? 0 : 1 + (k - 1 + r) % (nd2 - 1);
 }
 
-// One block-step of a sweep inside a CTA: (optionally) all pairs inside each
-// of the two slots, then all pairs between slot 0 and slot 1.
+// All pairs inside each slot (step 0 of a sweep): round 0 = the inner pairs of
+// every quad (two quads per warp), rounds 1 .. nq2-1 = a round robin over the
+// quads of each slot (a quad drawn against the dummy only advances its stamp).
+// Returns the stamp every quad holds afterwards.
 template <int RPL, int NT>
-__device__ void step_rounds(const Slots &S, int w, bool internal, int warp, int lane, double tol2, int &cnt) {
-    constexpr int kUpdWarps = NT / 32;
-    const int nd = w >> 1;
-    if (internal) {
-        // inner pairs of all 2*nd duos, two duos per warp (an odd last one is paired with itself)
-        for (int t = 2 * warp; t < 2 * nd; t += 2 * kUpdWarps) {
-            const int t1 = (t + 1 < 2 * nd) ? t + 1 : t;
-            cnt += duo_inner2<RPL>(S, nd, t, t1, lane, tol2);
-        }
-        __syncthreads();
-        const int nd2 = nd + (nd & 1);
-        const int half = nd2 >> 1;
-        for (int r = 0; r < nd2 - 1; ++r) {
-            for (int t = warp; t < 2 * half; t += kUpdWarps) {
-                const int slot = t / half, k = t - slot * half;
-                const int u = rr_elem(k, r, nd2), v = rr_elem(nd2 - 1 - k, r, nd2);
-                if (u < nd && v < nd) cnt += duo_pair<RPL>(S, slot, u, slot, v, lane, tol2);
+__device__ int internal_rounds(const Slots &S, int *stamp, int nq, int warp, int lane, double tol2, int &cnt,
+                               int &tmo) {
+    constexpr int kWarps = NT / 32;
+    for (int t = 2 * warp; t < 2 * nq; t += 2 * kWarps) {
+        const int sa = t / nq, qa = t - sa * nq, sb = (t + 1) / nq, qb = (t + 1) - sb * nq;
+        double2 A[4][RPL], B[4][RPL];
+        double a[4], b[4];
+        load_quad<RPL>(S, sa, qa, lane, A, a);
+        load_quad<RPL>(S, sb, qb, lane, B, b);
+        cnt += quad_inner2<RPL>(A, a, B, b, lane, tol2);
+        store_quad<RPL>(S, sa, qa, lane, A, a);
+        store_quad<RPL>(S, sb, qb, lane, B, b);
+        set_stamp(&stamp[sa * 8 + qa], 1, lane);
+        set_stamp(&stamp[sb * 8 + qb], 1, lane);
+    }
+    const int nq2 = nq + (nq & 1);
+    const int half = nq2 >> 1;
+    for (int r = 0; r < nq2 - 1; ++r) {
+        const int R = r + 1;
+        for (int t = warp; t < 2 * half; t += kWarps) {
+            const int slot = t / half, k = t - slot * half;
+            const int u = rr_elem(k, r, nq2), v = rr_elem(nq2 - 1 - k, r, nq2);
+            if (u < nq && v < nq) {
+                wait_stamp(&stamp[slot * 8 + u], R, lane, tmo);
+                wait_stamp(&stamp[slot * 8 + v], R, lane, tmo);
+                double2 P[4][RPL], Q[4][RPL];
+                double p[4], q[4];
+                load_quad<RPL>(S, slot, u, lane, P, p);
+                load_quad<RPL>(S, slot, v, lane, Q, q);
+                cnt += quad_cross<RPL>(P, p, Q, q, lane, tol2);
+                store_quad<RPL>(S, slot, u, lane, P, p);
+                store_quad<RPL>(S, slot, v, lane, Q, q);
+                set_stamp(&stamp[slot * 8 + u], R + 1, lane);
+                set_stamp(&stamp[slot * 8 + v], R + 1, lane);
+            } else {
+                const int real = u < nq ? u : v;
+                if (real < nq) {
+                    wait_stamp(&stamp[slot * 8 + real], R, lane, tmo);
+                    set_stamp(&stamp[slot * 8 + real], R + 1, lane);
+                }
             }
-            __syncthreads();
         }
     }
-    for (int r = 0; r < nd; ++r) {
-        for (int t = warp; t < nd; t += kUpdWarps) {
-            int v = t + r;
-            if (v >= nd) v -= nd;
-            cnt += duo_pair<RPL>(S, 0, t, 1, v, lane, tol2);
-        }
-        __syncthreads();
-    }
+    return nq2;
 }
 
-// Exact squared norms of the 2w local columns (start of every sweep).
+// All pairs between slot 0 and slot 1: warp t keeps quad t of slot 0 in
+// registers for the whole step while the quads of slot 1 travel round the
+// warps (round r pairs it with quad (t + r) mod nq, which warp t+1 released).
+template <int RPL, int NT>
+__device__ void cross_rounds(const Slots &S, int *stamp, int nq, int R0, int warp, int lane, double tol2, int &cnt,
+                             int &tmo) {
+    if (warp >= nq) return;
+    const int t = warp;
+    double2 P[4][RPL];
+    double p[4];
+    wait_stamp(&stamp[t], R0, lane, tmo);
+    load_quad<RPL>(S, 0, t, lane, P, p);
+    for (int r = 0; r < nq; ++r) {
+        int v = t + r;
+        if (v >= nq) v -= nq;
+        double2 Q[4][RPL];
+        double q[4];
+        wait_stamp(&stamp[8 + v], R0 + r, lane, tmo);
+        load_quad<RPL>(S, 1, v, lane, Q, q);
+        cnt += quad_cross<RPL>(P, p, Q, q, lane, tol2);
+        store_quad<RPL>(S, 1, v, lane, Q, q);
+        set_stamp(&stamp[8 + v], R0 + r + 1, lane);
+    }
+    store_quad<RPL>(S, 0, t, lane, P, p);
+}
+
 template <int RPL, int NT>
 __device__ void recompute_norms(const Slots &S, int w, int warp, int lane) {
     constexpr int kUpdWarps = NT / 32;
@@ -401,7 +480,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
     const int R = trans ? 2 * cr : 2 * cl;
     const int C = trans ? 2 * cl : 2 * cr;
     const int D = C >> 1;
-    const int w = ((C + 7) & ~7) >> 2;
+    const int w = ((C + 15) & ~15) >> 2;  // C padded to a multiple of 16: four blocks of whole quads
     const int idx0 = crank * w;
     const int nidx = max(0, min(D, idx0 + w) - idx0);
 
@@ -410,6 +489,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
         sc->nrot[0] = 0;
         sc->nrot[1] = 0;
         sc->nonfinite = 0;
+        sc->timeout = 0;
     }
     if (tid < 16) sc->gate[tid] = __ldg(p.gates + (size_t)pr.gate * 16 + tid);
     __syncthreads();
@@ -477,6 +557,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
 
     // ---- phase 2: one-sided Jacobi sweeps over the cluster
     int parity = 0;
+    int tmo = 0;
     bool converged = false;
     for (int sweep = 0; sweep < p.max_sweeps; ++sweep) {
         const int sb = sweep & 1;
@@ -484,7 +565,12 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
         recompute_norms<RPL, NT>(S, w, warp, lane);
         int cnt = 0;
         for (int step = 0; step < 3; ++step) {
-            step_rounds<RPL, NT>(S, w, step == 0, warp, lane, p.tol2, cnt);
+            if (tid < 16) sc->stamp[tid] = 0;
+            __syncthreads();
+            int R0 = 0;
+            if (step == 0) R0 = internal_rounds<RPL, NT>(S, sc->stamp, w >> 2, warp, lane, p.tol2, cnt, tmo);
+            cross_rounds<RPL, NT>(S, sc->stamp, w >> 2, R0, warp, lane, p.tol2, cnt, tmo);
+            __syncthreads();
             if (step == 2 && lane == 0 && cnt) atomicAdd(&sc->nrot[sb], cnt);
             exchange_slots<NT>(cluster, S, stage, stage_nrm, crank, parity, w, tid);
             parity ^= 1;
@@ -495,6 +581,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
             break;
         }
     }
+
+    if (lane == 0 && tmo) atomicOr(&sc->timeout, 1);
 
     // ---- phase 3: singular values, ranks, keep rule
     for (int j = warp; j < 2 * w; j += kUpdWarps) {
@@ -529,8 +617,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
             rS[rk] = sv;
         }
     }
-    int remote_nonfinite = 0;
-    if (tid == 0) remote_nonfinite = *cluster.map_shared_rank(&sc->nonfinite, crank ^ 1);
+    int remote_nonfinite = 0, remote_timeout = 0;
+    if (tid == 0) {
+        remote_nonfinite = *cluster.map_shared_rank(&sc->nonfinite, crank ^ 1);
+        remote_timeout = *cluster.map_shared_rank(&sc->timeout, crank ^ 1);
+    }
     cluster.sync();  // (B) sorted spectrum complete in both CTAs
 
     if (tid == 0) {
@@ -564,6 +655,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
         if (crank == 0) {
             int st = converged ? 0 : MPSB_ST_NOCONV;
             if (sc->nonfinite | remote_nonfinite) st |= MPSB_ST_NONFINITE;
+            if (sc->timeout | remote_timeout) st |= MPSB_ST_TIMEOUT;
             const double disc = tot > 0.0 ? dropped / tot : 0.0;
             p.rec[pi] = PairRec{d1, d2, disc, keep, st};
             p.status[pr.out] = st;
@@ -667,27 +759,15 @@ size_t upd_workspace_bytes(int npairs, int chi_cap) {
 
 template <int RPL, int NT>
 static int launch_rpl(const Upd2Params &p, size_t smem, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
+    static size_t configured = 0;  // largest dynamic shared memory size enabled so far
+    if (smem > configured) {
         if (cudaFuncSetAttribute(update2q_fp64_kernel<RPL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return check_launch("cudaFuncSetAttribute(update2q)");
-        configured = true;
+        configured = smem;
     }
     update2q_fp64_kernel<RPL, NT><<<2 * p.npairs, NT, smem, s>>>(p);
     return check_launch("update2q_fp64_kernel");
-}
-
-// CTA size per rows-per-lane class; MPSB_UPD_THREADS=256|512 overrides (tuning).
-static int upd_threads(int rpl) {
-    static int forced = -1;
-    if (forced < 0) {
-        const char *e = getenv("MPSB_UPD_THREADS");
-        forced = e ? atoi(e) : 0;
-    }
-    if (forced == 256 || forced == 512) return forced;
-    (void)rpl;
-    return 256;
 }
 
 int launch_update2q(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const double2 *gates,
@@ -707,20 +787,20 @@ int launch_update2q(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs
     p.trunc = trunc;
     p.status = status;
     p.chi_cap = chi_cap;
-    const int rpl = (2 * chi_cap + 31) / 32;
+    // rows per lane: 1 (theta <= 32 rows), 2 (<= 64) or 4 (<= 128)
+    const int rpl = (2 * chi_cap <= 32) ? 1 : (2 * chi_cap <= 64) ? 2 : 4;
     p.rpad = 32 * rpl;
-    p.wmax = (((2 * chi_cap) + 7) & ~7) / 4;
+    p.wmax = (((2 * chi_cap) + 15) & ~15) / 4;
     p.tol2 = tol * tol;
     p.max_sweeps = max_sweeps;
     const size_t smem = upd_smem_bytes(p.wmax, p.rpad);
     int rc;
-    const bool big = upd_threads(rpl) == 512;
-    switch (rpl) {
-        case 1: rc = big ? launch_rpl<1, 512>(p, smem, stream) : launch_rpl<1, 256>(p, smem, stream); break;
-        case 2: rc = big ? launch_rpl<2, 512>(p, smem, stream) : launch_rpl<2, 256>(p, smem, stream); break;
-        case 3: rc = big ? launch_rpl<3, 512>(p, smem, stream) : launch_rpl<3, 256>(p, smem, stream); break;
-        default: rc = big ? launch_rpl<4, 512>(p, smem, stream) : launch_rpl<4, 256>(p, smem, stream); break;
-    }
+    if (rpl == 1)
+        rc = launch_rpl<1, kUpdThreads>(p, smem, stream);
+    else if (rpl == 2)
+        rc = launch_rpl<2, kUpdThreads>(p, smem, stream);
+    else
+        rc = launch_rpl<4, kUpdThreads>(p, smem, stream);
     if (rc != MPSB_OK) return rc;
     fold_norm_log_kernel<<<(npairs + 127) / 128, 128, 0, stream>>>(chains, pairs, npairs, p.rec);
     return check_launch("fold_norm_log_kernel");

@@ -84,7 +84,8 @@ enum mpsb_status_bits {
     MPSB_ST_OK = 0,
     MPSB_ST_NOCONV = 1,    /* Jacobi hit max_sweeps; result written anyway */
     MPSB_ST_NONFINITE = 2, /* theta held NaN or Inf                         */
-    MPSB_ST_BADDIM = 4     /* bond dimensions out of range; pair skipped    */
+    MPSB_ST_BADDIM = 4,    /* bond dimensions out of range; pair skipped    */
+    MPSB_ST_TIMEOUT = 8    /* a bounded intra-CTA wait gave up; result invalid */
 };
 
 enum mpsb_error {
