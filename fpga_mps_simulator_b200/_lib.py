@@ -23,7 +23,7 @@ _ERRORS = {-1: "EINVAL", -2: "ELAUNCH", -3: "EWORKSPACE", -4: "ENODEV"}
 EXPORTS = (
     "mpsb_version", "mpsb_last_error", "mpsb_update2q_workspace_bytes", "mpsb_update2q_batch",
     "mpsb_apply1q_batch", "mpsb_statevector", "mpsb_amplitude", "mpsb_expect_workspace_bytes",
-    "mpsb_expect_local", "mpsb_fp64_probe", "mpsb_update2q_batch_noalloc",
+    "mpsb_expect_local", "mpsb_fp64_probe", "mpsb_update2q_batch_noalloc", "mpsb_overlap",
 )
 
 
@@ -73,6 +73,7 @@ def _declare(lib):
         "mpsb_expect_local": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp, vp, sz, vp]),
         "mpsb_fp64_probe": (i32, [i64, i32, i32, vp, vp]),
         "mpsb_update2q_batch_noalloc": (i32, [vp, vp, i32, vp, i32, i32, dbl, i32, vp, vp, vp, vp, vp]),
+        "mpsb_overlap": (i32, [vp, vp, i32, i32, vp, vp, vp, sz, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

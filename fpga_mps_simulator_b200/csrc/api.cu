@@ -45,6 +45,7 @@ size_t expect_workspace_bytes(int nchains, int n, int chi_cap, int nctas);
 int launch_expect(const mpsb_chain *, int, int, int, const int32_t *, const int32_t *, const double2 *, int,
                   double *, void *, int, cudaStream_t);
 int launch_fp64_probe(long long iters, int blocks, int threads, double *sink, cudaStream_t s);
+int launch_overlap(const mpsb_chain *, const mpsb_chain *, int, int, double2 *, double *, void *, cudaStream_t);
 
 static int expect_ctas() {
     int dev = 0, sms = 148;
@@ -160,6 +161,21 @@ int mpsb_expect_local(const mpsb_chain *chains, int nchains, int n, int chi_cap,
     if (rc) return rc;
     return launch_expect(chains, nchains, n, chi_cap, sites, two_site, reinterpret_cast<const double2 *>(ops),
                          nterms, out, workspace, nctas, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mpsb_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap, mpsb_c128 *out, double *out_log,
+                 void *workspace, size_t workspace_bytes, mpsb_stream_t stream) {
+    if (!a || !b || !out || !out_log || !workspace) return set_error(MPSB_EINVAL, "null pointer argument");
+    if (n < 1) return set_error(MPSB_EINVAL, "n=%d < 1", n);
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    const size_t need = 2 * (size_t)chi_cap * chi_cap * sizeof(double2);
+    if (workspace_bytes < need)
+        return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_overlap(a, b, n, chi_cap, reinterpret_cast<double2 *>(out), out_log, workspace,
+                          reinterpret_cast<cudaStream_t>(stream));
 }
 
 int mpsb_fp64_probe(int64_t iters, int blocks, int threads, double *sink, mpsb_stream_t stream) {

@@ -403,6 +403,75 @@ int launch_expect(const mpsb_chain *chains, int nchains, int n, int chi_cap, con
     return check_launch("terms_kernel");
 }
 
+// ------------------------------------------------------------- overlap
+// <a|b> of two chains of equal length: E_{k+1}[c, d] = sum_{x,y,s}
+// conj(A_k[x,s,c]) E_k[x,y] B_k[y,s,d], rescaled by its largest magnitude
+// each site (the scale is returned as a log).  One CTA; T in global scratch.
+__global__ void overlap_kernel(const mpsb_chain *pa, const mpsb_chain *pb, int n, int chi_cap, double2 *out,
+                               double *out_log, double2 *tscr) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    double2 *E = reinterpret_cast<double2 *>(sm);
+    double2 *En = E + chi_cap * chi_cap;
+    __shared__ double red[32];
+    const int tid = threadIdx.x, nth = blockDim.x;
+    const mpsb_chain a = *pa, b = *pb;
+    if (tid == 0) E[0] = make_double2(1.0, 0.0);
+    double lg = 0.0;
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        const int cla = a.bonds[k], cra = a.bonds[k + 1], clb = b.bonds[k], crb = b.bonds[k + 1];
+        const double2 *A = reinterpret_cast<const double2 *>(a.sites + (size_t)k * a.slot_elems);
+        const double2 *B = reinterpret_cast<const double2 *>(b.sites + (size_t)k * b.slot_elems);
+        for (int e = tid; e < cla * 2 * crb; e += nth) {  // T[x, t, d] = sum_y E[x, y] B[y, t, d]
+            const int x = e / (2 * crb), rem = e - x * 2 * crb;
+            double2 acc = make_double2(0, 0);
+            for (int y = 0; y < clb; ++y) acc = c_fma(E[x * clb + y], B[(size_t)y * 2 * crb + rem], acc);
+            tscr[e] = acc;
+        }
+        __threadfence_block();
+        __syncthreads();
+        double part = 0.0;
+        for (int e = tid; e < cra * crb; e += nth) {  // E'[c, d] = sum_{x,s} conj(A[x,s,c]) T[x,s,d]
+            const int c = e / crb, d = e - c * crb;
+            double2 acc = make_double2(0, 0);
+            for (int x = 0; x < cla; ++x) {
+                acc = c_cfma(A[(size_t)(2 * x) * cra + c], tscr[(size_t)(2 * x) * crb + d], acc);
+                acc = c_cfma(A[(size_t)(2 * x + 1) * cra + c], tscr[(size_t)(2 * x + 1) * crb + d], acc);
+            }
+            En[e] = acc;
+            part = fmax(part, c_abs2(acc));
+        }
+        // block max
+        for (int o = 16; o > 0; o >>= 1) part = fmax(part, __shfl_xor_sync(0xffffffffu, part, o));
+        if ((tid & 31) == 0) red[tid >> 5] = part;
+        __syncthreads();
+        double mx = 0.0;
+        for (int q = 0; q < nth / 32; ++q) mx = fmax(mx, red[q]);
+        const double sc = mx > 0.0 ? rsqrt(mx) : 1.0;
+        if (mx > 0.0) lg -= log(sc);
+        for (int e = tid; e < cra * crb; e += nth) E[e] = c_scale(En[e], sc);
+        __syncthreads();
+    }
+    if (tid == 0) {
+        out[0] = E[0];
+        out_log[0] = lg + *a.norm_log + *b.norm_log;
+    }
+}
+
+int launch_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap, double2 *out, double *out_log,
+                   void *ws, cudaStream_t s) {
+    const size_t smem = 2 * (size_t)chi_cap * chi_cap * sizeof(double2);
+    static size_t configured = 0;
+    if (smem > configured) {
+        if (cudaFuncSetAttribute(overlap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return check_launch("cudaFuncSetAttribute(overlap)");
+        configured = smem;
+    }
+    overlap_kernel<<<1, 256, smem, s>>>(a, b, n, chi_cap, out, out_log, reinterpret_cast<double2 *>(ws));
+    return check_launch("overlap_kernel");
+}
+
 // ------------------------------------------------------------- FP64 probe
 // Eight independent FMA chains per thread; the caller times the launch.
 __global__ void fp64_probe_kernel(long long iters, double *sink) {

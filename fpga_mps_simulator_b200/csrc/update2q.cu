@@ -24,6 +24,7 @@
 //   keeps the product U S Vh exact to rounding (checked against the reference
 //   over full circuits).
 #include "mpsb_common.cuh"
+#include "contract_tf32.cuh"
 
 #include <cstdio>
 #include <cstdlib>
@@ -33,6 +34,7 @@ namespace mpsb {
 // 256 threads per CTA: eight warps, one column-quad task per warp and round
 // at chi = 64 (a slot holds up to eight quads), up to 255 registers each.
 constexpr int kUpdThreads = 256;
+constexpr double kMixedCutoffFloor = 1e-6;
 
 struct Upd2Params {
     const mpsb_chain *chains;
@@ -51,6 +53,7 @@ struct Upd2Params {
     int rpad;             // row capacity of a column (multiple of 32)
     double tol2;          // squared Jacobi tolerance
     int max_sweeps;
+    double cut_floor;     // lower bound on the relative cutoff (mixed form: theta's rounding floor)
 };
 
 struct CtaScalars {
@@ -62,12 +65,25 @@ struct CtaScalars {
     double div;
     double2 gate[16];
     int stamp[16];  // per column quad (slot * 8 + quad): rounds completed in the current step
+    uint64_t mbar;            // tensor-core completion barrier (mixed form)
+    uint32_t tmem;            // TMEM base address (mixed form)
 };
+static_assert(sizeof(CtaScalars) <= 384, "CTA scalars exceed their reserved header");
 
 // Dynamic shared memory: scalars, slots, staging block, spectrum/rank arrays, norms.
 __host__ __device__ inline size_t upd_smem_bytes(int wmax, int rpad) {
     return 384 + (size_t)3 * wmax * rpad * sizeof(double2) + (size_t)2 * wmax * sizeof(double) +
            (size_t)4 * wmax * sizeof(double) + (size_t)4 * wmax * sizeof(int) + (size_t)3 * wmax * sizeof(double);
+}
+// The mixed form stages tensor-core operands from the slot area onwards
+// (hi and lo tf32 of a 128 x kpad A operand and an npad x kpad B operand);
+// everything it overlaps is written only after the contraction.
+__host__ __device__ inline size_t upd_smem_bytes_mixed(int wmax, int rpad, int chi_cap) {
+    const size_t kpad = (size_t)((chi_cap + 7) & ~7);
+    const size_t npad = (size_t)(((2 * wmax) + 15) & ~15) < 16 ? 16 : (size_t)(((2 * wmax) + 15) & ~15);
+    const size_t ops = 2 * 128 * kpad * 4 + 2 * npad * kpad * 4;
+    const size_t base = upd_smem_bytes(wmax, rpad);
+    return (384 + ops > base) ? 384 + ops : base;
 }
 
 // ------------------------------------------------------------- rotations
@@ -431,7 +447,7 @@ __device__ void exchange_slots(cg::cluster_group &cluster, const Slots &S, doubl
     __syncthreads();
 }
 
-template <int RPL, int NT>
+template <int RPL, int NT, bool MIXED>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
     update2q_fp64_kernel(const Upd2Params p) {
     constexpr int kUpdThreads = NT;
@@ -484,7 +500,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
     const int idx0 = crank * w;
     const int nidx = max(0, min(D, idx0 + w) - idx0);
 
-    for (int e = tid; e < 2 * wmax * rpad; e += kUpdThreads) X[e] = make_double2(0.0, 0.0);
+    if (!MIXED)
+        for (int e = tid; e < 2 * wmax * rpad; e += kUpdThreads) X[e] = make_double2(0.0, 0.0);
     if (tid == 0) {
         sc->nrot[0] = 0;
         sc->nrot[1] = 0;
@@ -495,7 +512,18 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
     __syncthreads();
 
     // ---- phase 1: theta for this CTA's columns, into X (smem) and X0 (workspace)
-    {
+    if constexpr (MIXED) {
+        const double2 *A = reinterpret_cast<const double2 *>(ch.sites + (size_t)i * ch.slot_elems);
+        const double2 *B = reinterpret_cast<const double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
+        double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
+        int nonfin = 0;
+        const bool ok = contract_mixed<NT>(reinterpret_cast<unsigned char *>(X), &sc->mbar, &sc->tmem, A, B,
+                                           sc->gate, cl, cm, cr, trans, idx0, nidx, C, w, wmax, rpad, X, x0, tid,
+                                           nonfin);
+        if (nonfin) atomicOr(&sc->nonfinite, 1);
+        if (!ok && tid == 0) sc->timeout = 1;
+        __threadfence();
+    } else {
         const double2 *g = sc->gate;
         const double2 *A = reinterpret_cast<const double2 *>(ch.sites + (size_t)i * ch.slot_elems);
         const double2 *B = reinterpret_cast<const double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
@@ -625,7 +653,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
     cluster.sync();  // (B) sorted spectrum complete in both CTAs
 
     if (tid == 0) {
-        const double thr = ch.cutoff * Ssorted[0];
+        const double thr = fmax(ch.cutoff, p.cut_floor) * Ssorted[0];
         int cnt = 0;
         double tot = 0.0;
         for (int k = 0; k < C; ++k) {
@@ -757,22 +785,22 @@ size_t upd_workspace_bytes(int npairs, int chi_cap) {
     return align256((size_t)npairs * sizeof(PairRec)) + (size_t)npairs * x0_stride * sizeof(double2);
 }
 
-template <int RPL, int NT>
+template <int RPL, int NT, bool MIXED>
 static int launch_rpl(const Upd2Params &p, size_t smem, cudaStream_t s) {
     static size_t configured = 0;  // largest dynamic shared memory size enabled so far
     if (smem > configured) {
-        if (cudaFuncSetAttribute(update2q_fp64_kernel<RPL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(update2q_fp64_kernel<RPL, NT, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return check_launch("cudaFuncSetAttribute(update2q)");
         configured = smem;
     }
-    update2q_fp64_kernel<RPL, NT><<<2 * p.npairs, NT, smem, s>>>(p);
-    return check_launch("update2q_fp64_kernel");
+    update2q_fp64_kernel<RPL, NT, MIXED><<<2 * p.npairs, NT, smem, s>>>(p);
+    return check_launch("update2q kernel");
 }
 
-int launch_update2q(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const double2 *gates,
-                    int chi_cap, double tol, int max_sweeps, void *ws, double *spectra, int32_t *kept,
-                    double *trunc, int32_t *status, cudaStream_t stream) {
+static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+                                const double2 *gates, int chi_cap, double tol, int max_sweeps, void *ws,
+                                double *spectra, int32_t *kept, double *trunc, int32_t *status, cudaStream_t stream) {
     if (npairs == 0) return MPSB_OK;
     Upd2Params p;
     p.chains = chains;
@@ -793,17 +821,43 @@ int launch_update2q(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs
     p.wmax = (((2 * chi_cap) + 15) & ~15) / 4;
     p.tol2 = tol * tol;
     p.max_sweeps = max_sweeps;
-    const size_t smem = upd_smem_bytes(p.wmax, p.rpad);
+    // 3xTF32 theta carries relative errors near 1e-7, so singular values below
+    // ~1e-6 S[0] are rounding noise: the mixed form never keeps them
+    p.cut_floor = mixed ? kMixedCutoffFloor : 0.0;
+    const size_t smem = mixed ? upd_smem_bytes_mixed(p.wmax, p.rpad, chi_cap) : upd_smem_bytes(p.wmax, p.rpad);
     int rc;
-    if (rpl == 1)
-        rc = launch_rpl<1, kUpdThreads>(p, smem, stream);
-    else if (rpl == 2)
-        rc = launch_rpl<2, kUpdThreads>(p, smem, stream);
-    else
-        rc = launch_rpl<4, kUpdThreads>(p, smem, stream);
+    if (mixed) {
+        if (rpl == 1)
+            rc = launch_rpl<1, kUpdThreads, true>(p, smem, stream);
+        else if (rpl == 2)
+            rc = launch_rpl<2, kUpdThreads, true>(p, smem, stream);
+        else
+            rc = launch_rpl<4, kUpdThreads, true>(p, smem, stream);
+    } else {
+        if (rpl == 1)
+            rc = launch_rpl<1, kUpdThreads, false>(p, smem, stream);
+        else if (rpl == 2)
+            rc = launch_rpl<2, kUpdThreads, false>(p, smem, stream);
+        else
+            rc = launch_rpl<4, kUpdThreads, false>(p, smem, stream);
+    }
     if (rc != MPSB_OK) return rc;
     fold_norm_log_kernel<<<(npairs + 127) / 128, 128, 0, stream>>>(chains, pairs, npairs, p.rec);
     return check_launch("fold_norm_log_kernel");
+}
+
+int launch_update2q(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const double2 *gates,
+                    int chi_cap, double tol, int max_sweeps, void *ws, double *spectra, int32_t *kept,
+                    double *trunc, int32_t *status, cudaStream_t stream) {
+    return launch_update2q_impl(false, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
+                                trunc, status, stream);
+}
+
+int launch_update2q_mixed(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const double2 *gates,
+                          int chi_cap, double tol, int max_sweeps, void *ws, double *spectra, int32_t *kept,
+                          double *trunc, int32_t *status, cudaStream_t stream) {
+    return launch_update2q_impl(true, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
+                                trunc, status, stream);
 }
 
 }  // namespace mpsb

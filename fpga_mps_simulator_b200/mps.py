@@ -31,7 +31,7 @@ import torch
 from . import _lib
 from .gates import GATE_MATRICES, permute_2q
 
-__all__ = ["MPSState", "MPSBatch", "PairBatch", "PRECISIONS", "validate_pairs"]
+__all__ = ["MPSState", "MPSBatch", "PairBatch", "PRECISIONS", "validate_pairs", "overlap", "infidelity"]
 
 PRECISIONS = {"fp64": _lib.FP64, "complex128": _lib.FP64, "mixed": _lib.MIXED_TF32X3,
               "tf32x3": _lib.MIXED_TF32X3}
@@ -347,6 +347,28 @@ class MPSBatch:
                                          ws.data_ptr(), ws.numel(), self._stream())
         _lib.check(rc, "mpsb_expect_local")
         return out.cpu().numpy().reshape(nch, len(terms))
+
+
+def overlap(a: "MPSBatch", ca: int, b: "MPSBatch", cb: int) -> Tuple[complex, float]:
+    """<a_ca | b_cb> as (mantissa, log_scale), norm_log of both chains included."""
+    if a.ns[ca] != b.ns[cb]:
+        raise ValueError("overlap needs chains of equal length")
+    cap = max(a.chi_cap, b.chi_cap)
+    out = torch.empty(1, dtype=torch.complex128, device=a.device)
+    lg = torch.empty(1, dtype=torch.float64, device=a.device)
+    ws = torch.empty(2 * cap * cap * 16, dtype=torch.uint8, device=a.device)
+    rc = a._lib.mpsb_overlap(a.chain_ptr(ca), b.chain_ptr(cb), a.ns[ca], cap, out.data_ptr(), lg.data_ptr(),
+                             ws.data_ptr(), ws.numel(), _stream_handle(a.device))
+    _lib.check(rc, "mpsb_overlap")
+    return complex(out.item()), float(lg.item())
+
+
+def infidelity(a: "MPSState", b: "MPSState") -> float:
+    """1 - |<a|b>|^2 / (<a|a><b|b>) of two single-chain states, on the device."""
+    ab, lab = overlap(a._b, 0, b._b, 0)
+    aa, laa = overlap(a._b, 0, a._b, 0)
+    bb, lbb = overlap(b._b, 0, b._b, 0)
+    return 1.0 - abs(ab) ** 2 / (aa.real * bb.real) * math.exp(2 * lab - laa - lbb)
 
 
 _PAULI = {"I": np.eye(2, dtype=np.complex128), "X": GATE_MATRICES["x"], "Y": GATE_MATRICES["y"],

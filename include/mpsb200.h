@@ -77,7 +77,9 @@ typedef struct {
 
 enum mpsb_precision {
     MPSB_FP64 = 0,        /* complex128 end to end (the drop-in form)                    */
-    MPSB_MIXED_TF32X3 = 1 /* theta by 3xTF32 complex-3M tensor-core GEMMs; FP64 SVD       */
+    MPSB_MIXED_TF32X3 = 1 /* theta by 3xTF32 complex-3M tensor-core GEMMs (tcgen05), FP64
+                             Jacobi SVD; singular values below 1e-6 S[0] (theta's rounding
+                             floor) are never kept, whatever the cutoff                 */
 };
 
 enum mpsb_status_bits {
@@ -177,6 +179,15 @@ MPSB_API int mpsb_expect_local(const mpsb_chain *chains, int nchains, int n, int
                       const int32_t *sites, const int32_t *two_site, const mpsb_c128 *ops,
                       int nterms, double *out, void *workspace, size_t workspace_bytes,
                       mpsb_stream_t stream);
+
+/* Overlap <a|b> of two chains of n sites (both device pointers), returned
+ * as out * exp(out_log) with the norm_log of both chains included, so that
+ * <a|b> matches the inner product of the two get_statevector() vectors
+ * (mps_core.py:433-461 convention).  workspace: 2 * chi_cap^2 complex128.
+ * No reference counterpart: used to report the state infidelity of the
+ * mixed-precision form against the FP64 form. */
+MPSB_API int mpsb_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap, mpsb_c128 *out,
+                          double *out_log, void *workspace, size_t workspace_bytes, mpsb_stream_t stream);
 
 /* FP64 FMA throughput probe: `blocks` x `threads` threads each run eight
  * independent FMA chains of `iters` steps (16 * iters flops per thread).

@@ -270,6 +270,30 @@ class OracleMPS:
         return shots
 
 
+def mps_overlap(sites_a, sites_b, log_a: float = 0.0, log_b: float = 0.0):
+    """<a|b> of two MPS given as lists of (chi_l, 2, chi_r) tensors, as
+    (mantissa, log_scale) with <a|b> = mantissa * exp(log_scale); the norm_log
+    factors of both states are included."""
+    e = np.ones((1, 1), np.complex128)
+    acc = 0.0
+    for a, b in zip(sites_a, sites_b):
+        e = np.einsum("xsc,xsd->cd", a.conj(), np.einsum("xy,ysd->xsd", e, b))
+        s = float(np.max(np.abs(e)))
+        if s > 0:
+            e = e / s
+            acc += math.log(s)
+    return complex(e[0, 0]), acc + log_a + log_b
+
+
+def infidelity(sites_a, sites_b) -> float:
+    """1 - |<a|b>|^2 / (<a|a><b|b>) of two MPS (norm_log factors cancel)."""
+    ab, lab = mps_overlap(sites_a, sites_b)
+    aa, laa = mps_overlap(sites_a, sites_a)
+    bb, lbb = mps_overlap(sites_b, sites_b)
+    f = abs(ab) ** 2 / (aa.real * bb.real) * math.exp(2 * lab - laa - lbb)
+    return float(1.0 - f)
+
+
 # -- dense statevector helpers (exact references) ------------------------------
 def dense_zero_state(n: int) -> np.ndarray:
     """|0...0> as an (2,)*n tensor with axis k = qubit k."""
