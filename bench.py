@@ -70,6 +70,73 @@ def replay_dims(n: int, layer_sites, layer_kept):
     return out
 
 
+BATCH_CIRCUITS, BATCH_N, BATCH_DEPTH, BATCH_CHIS = 256, (20, 200), (10, 40), (16, 32, 64)
+
+
+def batching_leg(dev, steps: int, rank: int, max_over_ranks, precision: str = "mixed"):
+    """Many uneven circuits: 256 Haar brick-walls, n ~ U[20,200], depth ~ U[10,40],
+    chi_max from {16,32,64}, cutoff 1e-10.  The autotuned launch strategy is
+    captured in one CUDA graph and replayed (device-timed per full run); the
+    comparison is a one-circuit-at-a-time loop of per-layer launches."""
+    import torch
+    from fpga_mps_simulator_b200 import MPSBatch
+    from fpga_mps_simulator_b200.circuits import random_circuit_batch
+    from fpga_mps_simulator_b200.schedule import Runner, Schedule, autotune, last_timings
+
+    specs = random_circuit_batch(BATCH_CIRCUITS, seed=SEED + rank, n_range=BATCH_N, depth_range=BATCH_DEPTH,
+                                 chis=BATCH_CHIS)
+    b = MPSBatch([s.n for s in specs], [s.chi_max for s in specs], CUTOFF, precision=precision, device=dev)
+    sch = Schedule(b, [s.layers for s in specs])
+    n_upd = sch.updates()
+    init = b.snapshot()
+    best = autotune(sch, start=12, layers=4, repeats=2)
+    tuned = dict(last_timings)
+    r = Runner(sch, best)
+    r.capture()
+
+    def timed(fn):
+        b.restore(init)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e-3
+
+    timed(r.run)  # warm replay
+    run_s = [timed(r.run) for _ in range(steps)]
+    b.check_status()
+    graph_s = max_over_ranks(sum(run_s)) / steps
+    launches = r.launches_per_run()
+    r.release()
+
+    # one circuit at a time: each circuit's layers launched in turn, sized for that circuit
+    loop_plan = []
+    for c, s in enumerate(specs):
+        for L in s.layers:
+            loop_plan.append(b.make_pairs(np.full(len(L.sites), c, np.int32), L.sites, L.gates))
+
+    def loop():
+        k = 0
+        for s in specs:
+            for _ in s.layers:
+                b.run_pairs(loop_plan[k], chi_cap=s.chi_max)
+                k += 1
+
+    loop_s = max_over_ranks(timed(loop))
+    b.check_status()
+    return {"workload": (f"{BATCH_CIRCUITS} Haar brick-wall circuits, n~U{list(BATCH_N)}, "
+                         f"depth~U{list(BATCH_DEPTH)}, chi_max in {list(BATCH_CHIS)}, cutoff {CUTOFF:g}, "
+                         f"{precision} form"),
+            "updates_per_run": n_upd, "strategy": best, "launches_per_run": launches,
+            "autotune_ms": {k: round(v, 3) for k, v in tuned.items()},
+            "graph_updates_per_s": round(n_upd / graph_s, 3), "graph_s_per_run": round(graph_s, 4),
+            "loop_updates_per_s": round(n_upd / loop_s, 3), "loop_s_per_run": round(loop_s, 4),
+            "speedup_vs_loop": round(loop_s / graph_s, 3),
+            "note": "graph = whole run captured as one CUDA graph; loop = one launch per circuit layer"}
+
+
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clock / throttle-reason samples taken while the timed region runs."""
@@ -230,7 +297,8 @@ def run_ours(args) -> None:
 
     def measure(precision: str, timed: bool):
         """Warm-up, then K device-timed steps of one form; returns stats and the final state."""
-        batch = MPSBatch([N_SITES], [CHI], [CUTOFF], precision=precision, device=dev)
+        tol = args.mixed_tol if precision == "mixed" else 0.0
+        batch = MPSBatch([N_SITES], [CHI], [CUTOFF], precision=precision, device=dev, tol=tol)
         pbs = [batch.make_pairs(np.zeros(len(L.sites), np.int32), L.sites, L.gates) for L in layers]
         for _ in range(args.warmup):
             reset(batch)
@@ -335,6 +403,10 @@ def run_ours(args) -> None:
         e2e = {"value": round(world * n_upd * args.steps / e2e_s, 3), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
+    batching = None
+    if not args.quick and not args.no_batching:
+        batching = batching_leg(dev, 2, rank, max_over_ranks)
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -361,6 +433,7 @@ def run_ours(args) -> None:
         "clocks": clk,
         "e2e": e2e,
         "per_update_path": single,
+        "batching": batching,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -375,7 +448,10 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed",
                     help="form of the headline value (the other form is reported beside it)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--quick", action="store_true", help="skip the e2e and per-update legs")
+    ap.add_argument("--quick", action="store_true", help="skip the e2e, per-update and batching legs")
+    ap.add_argument("--mixed-tol", type=float, default=0.0,
+                    help="Jacobi off-diagonal tolerance of the mixed form (0 = library default 1e-9)")
+    ap.add_argument("--no-batching", action="store_true", help="skip the 256-circuit batching leg")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -214,19 +214,36 @@ class MPSBatch:
     def make_pairs(self, chain_idx, sites, gates, record_spectra: bool = False) -> PairBatch:
         return PairBatch(self, chain_idx, sites, gates, record_spectra)
 
-    def run_pairs(self, pb: PairBatch, precision: Optional[str] = None) -> None:
-        """Launch one batched update (asynchronous, stream-ordered, graph-capturable)."""
+    def run_pairs(self, pb: PairBatch, precision: Optional[str] = None, chi_cap: Optional[int] = None,
+                  workspace: Optional[_Workspace] = None, stream: Optional[torch.cuda.Stream] = None) -> None:
+        """Launch one batched update (asynchronous, stream-ordered, graph-capturable).
+
+        ``chi_cap`` may be lowered to the largest chi_max of the chains this
+        launch touches (smaller shared memory per CTA); launches running
+        concurrently on different ``stream``s need their own ``workspace``.
+        """
         if pb.npairs == 0:
             return
         prec = PRECISIONS[precision or self.precision]
-        need = self._lib.mpsb_update2q_workspace_bytes(pb.npairs, self.chi_cap)
-        ws = self._ws.get(need)
+        cap = self.chi_cap if chi_cap is None else int(chi_cap)
+        need = self._lib.mpsb_update2q_workspace_bytes(pb.npairs, cap)
+        ws = (workspace or self._ws).get(need)
+        handle = (stream or torch.cuda.current_stream(self.device)).cuda_stream
         rc = self._lib.mpsb_update2q_batch(
             self.table.data_ptr(), pb.pairs.data_ptr(), pb.npairs, pb.gates.data_ptr(), prec,
-            self.chi_cap, self.tol, self.max_sweeps, ws.data_ptr(), ws.numel(),
-            _ptr(pb.spectra), pb.kept.data_ptr(), pb.trunc.data_ptr(), pb.status.data_ptr(),
-            self._stream())
+            cap, self.tol, self.max_sweeps, ws.data_ptr(), ws.numel(),
+            _ptr(pb.spectra), pb.kept.data_ptr(), pb.trunc.data_ptr(), pb.status.data_ptr(), handle)
         _lib.check(rc, "mpsb_update2q_batch")
+
+    def snapshot(self):
+        """Device copies of the mutable state (sites, bonds, norm_log, status)."""
+        return (self.sites.clone(), self.bonds.clone(), self.norm_logs.clone(), self.status_acc.clone())
+
+    def restore(self, snap) -> None:
+        self.sites.copy_(snap[0])
+        self.bonds.copy_(snap[1])
+        self.norm_logs.copy_(snap[2])
+        self.status_acc.copy_(snap[3])
 
     def apply_layer(self, chain_idx, sites, gates, precision: Optional[str] = None,
                     record_spectra: bool = False) -> PairBatch:
