@@ -24,6 +24,9 @@ EXPORTS = (
     "mpsb_version", "mpsb_last_error", "mpsb_update2q_workspace_bytes", "mpsb_update2q_batch",
     "mpsb_apply1q_batch", "mpsb_statevector", "mpsb_amplitude", "mpsb_expect_workspace_bytes",
     "mpsb_expect_local", "mpsb_fp64_probe", "mpsb_update2q_batch_noalloc", "mpsb_overlap",
+    "mpsb_update2q_tape_bytes", "mpsb_update2q_batch_taped", "mpsb_update2q_backward_workspace_bytes",
+    "mpsb_update2q_backward_batch", "mpsb_apply1q_backward_batch", "mpsb_mpo_grad_workspace_bytes",
+    "mpsb_mpo_energy_grad",
 )
 
 
@@ -74,6 +77,13 @@ def _declare(lib):
         "mpsb_fp64_probe": (i32, [i64, i32, i32, vp, vp]),
         "mpsb_update2q_batch_noalloc": (i32, [vp, vp, i32, vp, i32, i32, dbl, i32, vp, vp, vp, vp, vp]),
         "mpsb_overlap": (i32, [vp, vp, i32, i32, vp, vp, vp, sz, vp]),
+        "mpsb_update2q_tape_bytes": (sz, [i32, i32]),
+        "mpsb_update2q_batch_taped": (i32, [vp, vp, i32, vp, i32, i32, dbl, i32, vp, sz, vp, sz, vp, vp, vp, vp, vp]),
+        "mpsb_update2q_backward_workspace_bytes": (sz, [i32, i32]),
+        "mpsb_update2q_backward_batch": (i32, [vp, vp, vp, i32, vp, i32, vp, sz, vp, vp, sz, vp, vp]),
+        "mpsb_apply1q_backward_batch": (i32, [vp, vp, vp, i32, vp, i32, vp, vp]),
+        "mpsb_mpo_grad_workspace_bytes": (sz, [i32, i32, i32, i32]),
+        "mpsb_mpo_energy_grad": (i32, [vp, i32, i32, i32, vp, i32, vp, vp, vp, vp, sz, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

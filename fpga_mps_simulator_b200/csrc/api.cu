@@ -47,6 +47,18 @@ int launch_expect(const mpsb_chain *, int, int, int, const int32_t *, const int3
 int launch_fp64_probe(long long iters, int blocks, int threads, double *sink, cudaStream_t s);
 int launch_overlap(const mpsb_chain *, const mpsb_chain *, int, int, double2 *, double *, void *, cudaStream_t);
 
+size_t upd_tape_bytes(int npairs, int chi_cap);
+int launch_update2q_taped(bool, const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int,
+                          void *, void *, double *, int32_t *, double *, int32_t *, cudaStream_t);
+size_t bwd_workspace_bytes(int npairs, int chi_cap);
+int launch_update2q_backward(const mpsb_chain *, const mpsb_chain *, const mpsb_pair *, int, const double2 *, int,
+                             const void *, double2 *, void *, int32_t *, double, double, cudaStream_t);
+int launch_apply1q_backward(const mpsb_chain *, const mpsb_chain *, const mpsb_site_op *, int, const double2 *,
+                            double2 *, cudaStream_t);
+size_t mpo_grad_workspace_bytes(int nchains, int n, int chi_cap, int D);
+int launch_mpo_energy_grad(const mpsb_chain *, int, int, int, const double2 *, int, const double *, double *,
+                           const mpsb_chain *, void *, cudaStream_t);
+
 static int expect_ctas() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -176,6 +188,103 @@ int mpsb_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap, m
     if (rc) return rc;
     return launch_overlap(a, b, n, chi_cap, reinterpret_cast<double2 *>(out), out_log, workspace,
                           reinterpret_cast<cudaStream_t>(stream));
+}
+
+size_t mpsb_update2q_tape_bytes(int npairs, int chi_cap) {
+    if (npairs < 0 || chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT) return 0;
+    return upd_tape_bytes(npairs, chi_cap);
+}
+
+int mpsb_update2q_batch_taped(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const mpsb_c128 *gates,
+                              int precision, int chi_cap, double tol, int max_sweeps, void *workspace,
+                              size_t workspace_bytes, void *tape, size_t tape_bytes, double *spectra, int32_t *kept,
+                              double *trunc, int32_t *status, mpsb_stream_t stream) {
+    if (npairs < 0) return set_error(MPSB_EINVAL, "npairs=%d < 0", npairs);
+    if (npairs == 0) return MPSB_OK;
+    if (!chains || !pairs || !gates || !status || !workspace || !tape)
+        return set_error(MPSB_EINVAL, "null chains/pairs/gates/status/workspace/tape pointer");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3)
+        return set_error(MPSB_EINVAL, "unknown precision %d", precision);
+    const size_t need = upd_workspace_bytes(npairs, chi_cap);
+    if (workspace_bytes < need)
+        return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
+    const size_t tneed = upd_tape_bytes(npairs, chi_cap);
+    if (tape_bytes < tneed) return set_error(MPSB_EWORKSPACE, "tape of %zu bytes < %zu needed", tape_bytes, tneed);
+    if (((reinterpret_cast<uintptr_t>(workspace) | reinterpret_cast<uintptr_t>(tape)) & 255) != 0)
+        return set_error(MPSB_EINVAL, "workspace and tape must be 256-byte aligned");
+    int rc = check_device();
+    if (rc) return rc;
+    if (max_sweeps <= 0) max_sweeps = 40;
+    const bool mixed = precision == MPSB_MIXED_TF32X3;
+    if (tol <= 0.0) tol = mixed ? 1.0e-9 : 1.0e-14;
+    return launch_update2q_taped(mixed, chains, pairs, npairs, reinterpret_cast<const double2 *>(gates), chi_cap, tol,
+                                 max_sweeps, workspace, tape, spectra, kept, trunc, status,
+                                 reinterpret_cast<cudaStream_t>(stream));
+}
+
+size_t mpsb_update2q_backward_workspace_bytes(int npairs, int chi_cap) {
+    if (npairs < 0 || chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT) return 0;
+    return bwd_workspace_bytes(npairs, chi_cap);
+}
+
+int mpsb_update2q_backward_batch(const mpsb_chain *pre, const mpsb_chain *cot, const mpsb_pair *pairs, int npairs,
+                                 const mpsb_c128 *gates, int chi_cap, const void *tape, size_t tape_bytes,
+                                 mpsb_c128 *gate_grads, void *workspace, size_t workspace_bytes, int32_t *status,
+                                 mpsb_stream_t stream) {
+    if (npairs < 0) return set_error(MPSB_EINVAL, "npairs=%d < 0", npairs);
+    if (npairs == 0) return MPSB_OK;
+    if (!pre || !cot || !pairs || !gates || !tape || !workspace || !status)
+        return set_error(MPSB_EINVAL, "null pre/cot/pairs/gates/tape/workspace/status pointer");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    if (tape_bytes < upd_tape_bytes(npairs, chi_cap))
+        return set_error(MPSB_EWORKSPACE, "tape of %zu bytes < %zu needed", tape_bytes, upd_tape_bytes(npairs, chi_cap));
+    const size_t need = bwd_workspace_bytes(npairs, chi_cap);
+    if (workspace_bytes < need)
+        return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_update2q_backward(pre, cot, pairs, npairs, reinterpret_cast<const double2 *>(gates), chi_cap, tape,
+                                    reinterpret_cast<double2 *>(gate_grads), workspace, status, 1.0e-6, 1.0e-12,
+                                    reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mpsb_apply1q_backward_batch(const mpsb_chain *pre, const mpsb_chain *cot, const mpsb_site_op *ops, int nops,
+                                const mpsb_c128 *gates, int chi_cap, mpsb_c128 *gate_grads, mpsb_stream_t stream) {
+    if (nops < 0) return set_error(MPSB_EINVAL, "nops=%d < 0", nops);
+    if (nops == 0) return MPSB_OK;
+    if (!pre || !cot || !ops || !gates) return set_error(MPSB_EINVAL, "null pre/cot/ops/gates pointer");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_apply1q_backward(pre, cot, ops, nops, reinterpret_cast<const double2 *>(gates),
+                                   reinterpret_cast<double2 *>(gate_grads), reinterpret_cast<cudaStream_t>(stream));
+}
+
+size_t mpsb_mpo_grad_workspace_bytes(int nchains, int n, int chi_cap, int mpo_bond) {
+    if (nchains < 0 || n < 1 || chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT || mpo_bond < 1 || mpo_bond > 16) return 0;
+    return mpo_grad_workspace_bytes(nchains, n, chi_cap, mpo_bond);
+}
+
+int mpsb_mpo_energy_grad(const mpsb_chain *chains, int nchains, int n, int chi_cap, const mpsb_c128 *mpo,
+                         int mpo_bond, const double *weights, double *loss, const mpsb_chain *cot, void *workspace,
+                         size_t workspace_bytes, mpsb_stream_t stream) {
+    if (nchains < 0 || n < 1) return set_error(MPSB_EINVAL, "bad nchains/n");
+    if (nchains == 0) return MPSB_OK;
+    if (!chains || !mpo || !cot || !workspace) return set_error(MPSB_EINVAL, "null chains/mpo/cot/workspace pointer");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    if (mpo_bond < 1 || mpo_bond > 16) return set_error(MPSB_EINVAL, "mpo bond %d outside [1, 16]", mpo_bond);
+    const size_t need = mpo_grad_workspace_bytes(nchains, n, chi_cap, mpo_bond);
+    if (workspace_bytes < need)
+        return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_mpo_energy_grad(chains, nchains, n, chi_cap, reinterpret_cast<const double2 *>(mpo), mpo_bond,
+                                  weights, loss, cot, workspace, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int mpsb_fp64_probe(int64_t iters, int blocks, int threads, double *sink, mpsb_stream_t stream) {

@@ -64,6 +64,21 @@ struct PairRec {
     int32_t status;
 };
 
+// Adjoint tape of one two-site update, per pair, in double2 units with
+// Q = (2 chi_cap)^2:
+//   [0, Q)       X, the matrix the Jacobi orthogonalised (theta, or theta^H
+//                when chi_r > chi_l), R x C row-major
+//   [Q, 2Q)      the converged columns of X (u_k S_k) in decreasing order of
+//                S_k, column k at [Q + k R, Q + (k + 1) R)
+//   [2Q, 2Q+72)  144 doubles: S[0..128), then keep, the kept-norm divisor,
+//                R and C
+// rounded up to a multiple of 16 double2 (256 bytes).
+constexpr int kTapeMetaKeep = 128, kTapeMetaDiv = 129, kTapeMetaRows = 130, kTapeMetaCols = 131;
+__host__ __device__ inline long long tape_stride(int chi_cap) {
+    const long long q = (long long)(2 * chi_cap) * (2 * chi_cap);
+    return (2 * q + 72 + 15) & ~15LL;
+}
+
 }  // namespace mpsb
 
 // host-side error helpers (defined in api.cu)

@@ -54,6 +54,8 @@ struct Upd2Params {
     double tol2;          // squared Jacobi tolerance
     int max_sweeps;
     double cut_floor;     // lower bound on the relative cutoff (mixed form: theta's rounding floor)
+    double2 *tape_xs;     // tape mode: sorted Jacobi columns per pair (null = no tape)
+    double *tape_meta;    // tape mode: spectrum and kept count per pair
 };
 
 struct CtaScalars {
@@ -752,6 +754,26 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
             }
         }
     }
+    // tape: every column of the converged X in rank order (X_rho = u_rho S_rho)
+    // and the spectrum, for the adjoint; the forward result is unchanged
+    if (p.tape_xs) {
+        double2 *xs = p.tape_xs + (size_t)pi * p.x0_stride;
+        for (int e = tid; e < 2 * w * R; e += kUpdThreads) {
+            const int j = e / R, r = e - j * R;
+            const int rho = rank[j];
+            if (rho < C) xs[(size_t)rho * R + r] = colp(j)[r];
+        }
+        if (crank == 0) {
+            double *meta = p.tape_meta + (size_t)pi * p.x0_stride * 2;
+            for (int j = tid; j < 128; j += kUpdThreads) meta[j] = j < C ? Ssorted[j] : 0.0;
+            if (tid == 0) {
+                meta[kTapeMetaKeep] = (double)K;
+                meta[kTapeMetaDiv] = div;
+                meta[kTapeMetaRows] = (double)R;
+                meta[kTapeMetaCols] = (double)C;
+            }
+        }
+    }
     if (crank == 0 && tid == 0) ch.bonds[i + 1] = K;
     cluster.sync();
 }
@@ -780,6 +802,8 @@ __global__ void fold_norm_log_kernel(const mpsb_chain *chains, const mpsb_pair *
 // ------------------------------------------------------------------ host
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+size_t upd_tape_bytes(int npairs, int chi_cap) { return (size_t)npairs * tape_stride(chi_cap) * sizeof(double2); }
+
 size_t upd_workspace_bytes(int npairs, int chi_cap) {
     const size_t x0_stride = (size_t)(2 * chi_cap) * (2 * chi_cap);
     return align256((size_t)npairs * sizeof(PairRec)) + (size_t)npairs * x0_stride * sizeof(double2);
@@ -800,7 +824,8 @@ static int launch_rpl(const Upd2Params &p, size_t smem, cudaStream_t s) {
 
 static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
                                 const double2 *gates, int chi_cap, double tol, int max_sweeps, void *ws,
-                                double *spectra, int32_t *kept, double *trunc, int32_t *status, cudaStream_t stream) {
+                                double *spectra, int32_t *kept, double *trunc, int32_t *status, cudaStream_t stream,
+                                void *tape = nullptr) {
     if (npairs == 0) return MPSB_OK;
     Upd2Params p;
     p.chains = chains;
@@ -810,6 +835,15 @@ static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb
     p.rec = reinterpret_cast<PairRec *>(ws);
     p.x0 = reinterpret_cast<double2 *>(static_cast<char *>(ws) + align256((size_t)npairs * sizeof(PairRec)));
     p.x0_stride = (long long)(2 * chi_cap) * (2 * chi_cap);
+    p.tape_xs = nullptr;
+    p.tape_meta = nullptr;
+    if (tape) {  // theta, the sorted columns and the spectrum stay in the tape
+        const long long q = p.x0_stride;
+        p.x0 = reinterpret_cast<double2 *>(tape);
+        p.x0_stride = tape_stride(chi_cap);
+        p.tape_xs = p.x0 + q;
+        p.tape_meta = reinterpret_cast<double *>(p.x0 + 2 * q);
+    }
     p.spectra = spectra;
     p.kept = kept;
     p.trunc = trunc;
@@ -858,6 +892,13 @@ int launch_update2q_mixed(const mpsb_chain *chains, const mpsb_pair *pairs, int 
                           double *trunc, int32_t *status, cudaStream_t stream) {
     return launch_update2q_impl(true, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
                                 trunc, status, stream);
+}
+
+int launch_update2q_taped(bool mixed, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+                          const double2 *gates, int chi_cap, double tol, int max_sweeps, void *ws, void *tape,
+                          double *spectra, int32_t *kept, double *trunc, int32_t *status, cudaStream_t stream) {
+    return launch_update2q_impl(mixed, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
+                                trunc, status, stream, tape);
 }
 
 }  // namespace mpsb

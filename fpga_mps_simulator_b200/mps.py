@@ -181,12 +181,19 @@ class MPSBatch:
 
     # -- chain table ----------------------------------------------------------
     def _build_table(self) -> None:
+        self.table = self.make_table(self.sites, self.bonds)
+
+    def make_table(self, sites: torch.Tensor, bonds: torch.Tensor) -> torch.Tensor:
+        """Device chain table over ``sites`` / ``bonds`` laid out like this batch's own
+        (used for saved copies of the state and for cotangent arrays)."""
+        if sites.shape != self.sites.shape or bonds.shape != self.bonds.shape:
+            raise ValueError("a chain table needs sites and bonds shaped like the batch's")
         nch = len(self.ns)
         arr = (_lib.Chain * nch)()
-        sb = self.sites.element_size() * self.slot
+        sb = sites.element_size() * self.slot
         for c in range(nch):
-            arr[c].sites = self.sites.data_ptr() + int(self.site_off[c]) * sb
-            arr[c].bonds = self.bonds.data_ptr() + int(self.bond_off[c]) * 4
+            arr[c].sites = sites.data_ptr() + int(self.site_off[c]) * sb
+            arr[c].bonds = bonds.data_ptr() + int(self.bond_off[c]) * 4
             arr[c].norm_log = self.norm_logs.data_ptr() + c * 8
             arr[c].status_acc = self.status_acc.data_ptr() + c * 4
             arr[c].slot_elems = self.slot
@@ -194,8 +201,7 @@ class MPSBatch:
             arr[c].chi_max = self.chi_maxs[c]
             arr[c].cutoff = self.cutoffs[c]
         raw = np.frombuffer(bytes(arr), dtype=np.uint8).copy()
-        self.table = torch.from_numpy(raw).to(self.device)
-        self._table_host = arr
+        return torch.from_numpy(raw).to(self.device)
 
     def chain_ptr(self, c: int) -> int:
         return self.table.data_ptr() + c * C.sizeof(_lib.Chain)

@@ -189,6 +189,71 @@ MPSB_API int mpsb_expect_local(const mpsb_chain *chains, int nchains, int n, int
 MPSB_API int mpsb_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap, mpsb_c128 *out,
                           double *out_log, void *workspace, size_t workspace_bytes, mpsb_stream_t stream);
 
+/* ---------------------------------------------------------------- adjoint
+ * No reference counterpart: the reference engine has no gradients.  These
+ * entries differentiate exactly what mpsb_update2q_batch and
+ * mpsb_apply1q_batch compute, for a real loss L, with the cotangent of a
+ * complex array z taken as z_bar = dL/dRe z + i dL/dIm z.  Cotangents live in
+ * a second chain table `cot` whose sites array has the same slot layout as
+ * the state's (only its sites and slot_elems fields are read); the shapes
+ * come from the bonds of the `pre` table, the state before the op. */
+
+/* Bytes of tape mpsb_update2q_batch_taped writes for npairs pairs (theta as
+ * the Jacobi saw it, the converged Jacobi columns and the spectrum). */
+MPSB_API size_t mpsb_update2q_tape_bytes(int npairs, int chi_cap);
+
+/* mpsb_update2q_batch that also records the tape of every pair (pair q at
+ * q * mpsb_update2q_tape_bytes(1, chi_cap)).  The sites, bonds, norm_log and
+ * outputs are bit-identical to mpsb_update2q_batch's. */
+MPSB_API int mpsb_update2q_batch_taped(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+                                       const mpsb_c128 *gates, int precision, int chi_cap,
+                                       double tol, int max_sweeps,
+                                       void *workspace, size_t workspace_bytes,
+                                       void *tape, size_t tape_bytes,
+                                       double *spectra, int32_t *kept, double *trunc, int32_t *status,
+                                       mpsb_stream_t stream);
+
+/* Bytes of device workspace mpsb_update2q_backward_batch needs. */
+MPSB_API size_t mpsb_update2q_backward_workspace_bytes(int npairs, int chi_cap);
+
+/* Backward of one taped call: for every pair, the cotangents of the updated
+ * sites (slots i and i+1 of `cot`, shapes (chi_l, 2, keep) and (keep, 2, chi_r))
+ * are replaced in place by the cotangents of the sites before the update
+ * (shapes (chi_l, 2, chi_m) and (chi_m, 2, chi_r)).  `pre` must hold the
+ * sites and bonds the taped call started from.  The truncated-SVD backward
+ * includes the kept/discarded coupling terms with Lorentzian-broadened
+ * 1/(s_j^2 - s_i^2) (width 1e-12 s_0^2); discarded triplets below 1e-6 times
+ * the smallest kept value are treated as an exact null space.
+ * gate_grads (nullable): 16 complex128 per pair (row `out`), dL/dG.
+ * status: per-pair bits (BADDIM: tape and bonds disagree). */
+MPSB_API int mpsb_update2q_backward_batch(const mpsb_chain *pre, const mpsb_chain *cot, const mpsb_pair *pairs,
+                                          int npairs, const mpsb_c128 *gates, int chi_cap,
+                                          const void *tape, size_t tape_bytes, mpsb_c128 *gate_grads,
+                                          void *workspace, size_t workspace_bytes, int32_t *status,
+                                          mpsb_stream_t stream);
+
+/* Backward of mpsb_apply1q_batch: cot site <- G^H cot site in place, and
+ * (gate_grads nullable) 4 complex128 per op: dL/dG = sum cot' A^H. */
+MPSB_API int mpsb_apply1q_backward_batch(const mpsb_chain *pre, const mpsb_chain *cot, const mpsb_site_op *ops,
+                                         int nops, const mpsb_c128 *gates, int chi_cap, mpsb_c128 *gate_grads,
+                                         mpsb_stream_t stream);
+
+/* Bytes of device workspace mpsb_mpo_energy_grad needs. */
+MPSB_API size_t mpsb_mpo_grad_workspace_bytes(int nchains, int n, int chi_cap, int mpo_bond);
+
+/* Loss L_c = <psi_c|H|psi_c> / <psi_c|psi_c> of chains 0 .. nchains-1 (all of
+ * n sites) for a matrix-product operator H, and the cotangent of every site,
+ * weights[c] * 2 (H_eff A - L_c N_eff A) / <psi_c|psi_c>, written into `cot`.
+ * mpo: device, n * D * D * 4 complex128, W[k][a][b] a 2x2 operator (row-major,
+ * acting as |s><t| at [s][t]); state D-1 is the left boundary and state 0 the
+ * right one, with W[k][D-1][D-1] = W[k][0][0] = identity and no transition
+ * out of state 0 or into state D-1 (lower-triangular form).
+ * weights (nullable = all ones), loss (nullable): device, nchains doubles. */
+MPSB_API int mpsb_mpo_energy_grad(const mpsb_chain *chains, int nchains, int n, int chi_cap,
+                                  const mpsb_c128 *mpo, int mpo_bond, const double *weights, double *loss,
+                                  const mpsb_chain *cot, void *workspace, size_t workspace_bytes,
+                                  mpsb_stream_t stream);
+
 /* FP64 FMA throughput probe: `blocks` x `threads` threads each run eight
  * independent FMA chains of `iters` steps (16 * iters flops per thread).
  * The caller times the launch on `stream` to state the FP64 roofline.
