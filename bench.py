@@ -137,6 +137,177 @@ def batching_leg(dev, steps: int, rank: int, max_over_ranks, precision: str = "m
             "note": "graph = whole run captured as one CUDA graph; loop = one launch per circuit layer"}
 
 
+GRAD_N, GRAD_LAYERS, GRAD_VEC, GRAD_CHI, GRAD_CUT = 64, 8, 64, 32, 1e-12
+
+
+def _svd_flops(cl: int, cr: int) -> float:
+    m, n = 2 * cl, 2 * cr
+    if m < n:
+        m, n = n, m
+    return 4.0 * (14.0 * m * n * n + 8.0 * n ** 3)
+
+
+def hea_grad_flops(model, angles) -> float:
+    """Algorithmic flops of one energy + gradient step: per update the forward
+    (contraction, gate, nominal SVD) plus the backward counted as twice the
+    contraction and twice the SVD; dims replayed from an untimed forward."""
+    import torch
+    from fpga_mps_simulator_b200.adjoint import Step2Q
+    model._set_angles(angles)
+    model._reset()
+    b = model.batch
+    total = 0.0
+    for g in model.groups:
+        for st in g:
+            if isinstance(st, Step2Q):
+                bonds = b.bonds.cpu().numpy()
+                pairs = st.pb.pairs.cpu().numpy()
+                for c, i in pairs[:, :2]:
+                    o = int(b.bond_off[c]) + int(i)
+                    cl, cm, cr = int(bonds[o]), int(bonds[o + 1]), int(bonds[o + 2])
+                    contr = 32.0 * cl * cm * cr
+                    total += 3.0 * contr + 128.0 * cl * cr + 3.0 * _svd_flops(cl, cr)
+            model.engine._run(st)
+    torch.cuda.synchronize()
+    return total
+
+
+def gradient_leg(dev, steps: int, warmup: int, rank: int, max_over_ranks, cpu_workers: int = 0):
+    """Energy + adjoint gradient of 64 hardware-efficient-ansatz parameter vectors
+    (n=64, 8 layers of RY, RZ and brick-wall CZ, chi_max=32, transverse-field
+    Ising energy) per step, with per-layer checkpointing; both forms."""
+    import torch
+    from fpga_mps_simulator_b200.adjoint import HEAEnergy
+    from fpga_mps_simulator_b200.circuits import hea_angles
+    angles = torch.tensor(hea_angles(GRAD_N, GRAD_LAYERS, GRAD_VEC, SEED + rank), dtype=torch.float64, device=dev)
+    out, grads = {}, {}
+    flops = None
+    for prec in ("fp64", "mixed"):
+        model = HEAEnergy(GRAD_N, GRAD_LAYERS, GRAD_VEC, chi_max=GRAD_CHI, cutoff=GRAD_CUT, precision=prec,
+                          device=dev, checkpoint=True)
+        for _ in range(warmup):
+            model.energy_and_grad(angles)
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats(dev)
+        base_mem = torch.cuda.memory_allocated(dev)
+        model.engine.launches = 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            E, g = model.energy_and_grad(angles)
+        e1.record()
+        torch.cuda.synchronize()
+        sec = max_over_ranks(e0.elapsed_time(e1) * 1e-3) / steps
+        grads[prec] = (E.clone(), g.clone())
+        if flops is None:
+            flops = hea_grad_flops(model, angles)
+        out[prec] = {"s_per_grad_step": round(sec, 5), "grad_steps_per_s": round(1.0 / sec, 4),
+                     "param_vectors_per_s": round(GRAD_VEC / sec, 3),
+                     "launches_per_step": model.engine.launches // steps,
+                     "peak_mem_gb": round((torch.cuda.max_memory_allocated(dev) - base_mem) / 1e9, 3),
+                     "achieved_tflops": round(flops / sec / 1e12, 4)}
+        del model
+        torch.cuda.empty_cache()
+    (e64, g64), (emx, gmx) = grads["fp64"], grads["mixed"]
+    res = {"workload": (f"{GRAD_VEC} parameter vectors of a {GRAD_N}-qubit hardware-efficient ansatz, "
+                        f"{GRAD_LAYERS} layers (RY, RZ every site, CZ brick-wall), chi_max={GRAD_CHI}, "
+                        f"transverse-field Ising energy J=h=1; energy + adjoint gradient per step, "
+                        f"per-layer checkpointing"),
+           "fp64": out["fp64"], "mixed": out["mixed"],
+           "mixed_vs_fp64": {"max_abs_energy_diff": float(torch.max(torch.abs(emx - e64))),
+                             "max_rel_grad_diff": float(torch.max(torch.abs(gmx - g64)) / torch.max(torch.abs(g64)))},
+           "flops_per_step": flops}
+    if cpu_workers:
+        from oracle.cpu_baseline import make_pool, run_grad_parallel
+        pool = make_pool(cpu_workers)
+        try:
+            run_grad_parallel(8, 1, 4, GRAD_CUT, cpu_workers, pool=pool)
+            r = run_grad_parallel(GRAD_N, GRAD_LAYERS, GRAD_CHI, GRAD_CUT, cpu_workers, seed=SEED, pool=pool)
+        finally:
+            pool.close()
+            pool.join()
+        res["cpu_baseline"] = {"value": round(GRAD_VEC / r["vectors_per_s"], 3), "unit": "s/grad step",
+                               "cores": cpu_workers, "kind": "port",
+                               "sample": (f"{cpu_workers} single-BLAS-thread processes, one parameter vector each "
+                                          f"({r['wall_s']:.1f} s wall), CPU adjoint oracle (scipy gesdd); "
+                                          f"extrapolated to {GRAD_VEC} vectors")}
+    return res
+
+
+LARGE_N, LARGE_STEPS, LARGE_DT, LARGE_CHI, LARGE_CUT, LARGE_FD = 1000, 30, 0.05, 64, 1e-10, 20
+
+
+def large_leg(dev, precision: str = "fp64"):
+    """1000-qubit open XXZ chain (Jxy=1, Jz=0.5), 30 second-order Trotter steps of
+    dt=0.05 from a seeded random product state, chi_max=64, cutoff 1e-10: the
+    gradient of sum <Z_i Z_{i+1}> with respect to the 2000 initial Bloch angles
+    with per-Trotter-step checkpointing, its memory high-water, and central
+    differences (h=1e-5) on 20 sampled angles run as one 40-chain forward."""
+    import torch
+    from fpga_mps_simulator_b200 import MPSBatch
+    from fpga_mps_simulator_b200.adjoint import AdjointEngine, XXZInitialStateGradient
+    from fpga_mps_simulator_b200.circuits import random_product_angles, xxz_trotter_layers
+    from fpga_mps_simulator_b200.hamiltonians import zz_mpo
+    angles = random_product_angles(LARGE_N, SEED)
+    model = XXZInitialStateGradient(LARGE_N, LARGE_STEPS, LARGE_DT, 1.0, 0.5, chi_max=LARGE_CHI, cutoff=LARGE_CUT,
+                                    precision=precision, device=dev, checkpoint=True)
+    model.energy_and_grad(angles)  # warm-up
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats(dev)
+    base = torch.cuda.memory_allocated(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    energy, grad = model.energy_and_grad(angles)
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) * 1e-3
+    peak = torch.cuda.max_memory_allocated(dev) - base
+    bonds = model.batch.bond_dims(0)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    e_fwd = model.energy(angles)
+    f1.record()
+    torch.cuda.synchronize()
+    fwd_s = f0.elapsed_time(f1) * 1e-3
+    grad = grad.cpu().numpy()
+    del model
+    torch.cuda.empty_cache()
+    # central differences: 2 x 20 perturbed initial states as independent chains of one batch
+    rng = np.random.default_rng(SEED + 1)
+    flat = rng.choice(LARGE_N * 2, size=LARGE_FD, replace=False)
+    picks = [(int(f) // 2, int(f) % 2) for f in flat]
+    h = 1e-5
+    nch = 2 * LARGE_FD
+    b = MPSBatch([LARGE_N] * nch, LARGE_CHI, LARGE_CUT, precision=precision, device=dev)
+    th = np.repeat(angles[None], nch, 0)
+    for p, idx in enumerate(picks):
+        th[2 * p][idx] += h
+        th[2 * p + 1][idx] -= h
+    t = torch.tensor(th.reshape(-1, 2), dtype=torch.float64, device=dev)
+    b.sites.zero_()
+    b.sites[:, 0] = torch.cos(0.5 * t[:, 0]).to(torch.complex128)
+    b.sites[:, 1] = torch.exp(1j * t[:, 1]) * torch.sin(0.5 * t[:, 0])
+    for L in xxz_trotter_layers(LARGE_N, LARGE_STEPS, LARGE_DT, 1.0, 0.5):
+        ci = np.repeat(np.arange(nch, dtype=np.int32), len(L.sites))
+        si = np.tile(L.sites, nch)
+        b.apply_layer(ci, si, np.tile(L.gates, (nch, 1, 1)))
+    b.check_status()
+    es = AdjointEngine(b, zz_mpo(LARGE_N)).energy().cpu().numpy()
+    fd = (es[0::2] - es[1::2]) / (2 * h)
+    adj = np.array([grad[idx] for idx in picks])
+    err = np.abs(adj - fd)
+    del b
+    torch.cuda.empty_cache()
+    return {"workload": (f"{LARGE_N}-qubit XXZ (Jxy=1, Jz=0.5), {LARGE_STEPS} second-order Trotter steps dt={LARGE_DT}, "
+                         f"random product start, chi_max={LARGE_CHI}, cutoff {LARGE_CUT:g}, {precision}; "
+                         "d sum<ZZ> / d initial angles, per-Trotter-step checkpointing"),
+            "energy": energy, "energy_forward_only": e_fwd, "s_energy_and_grad": round(sec, 4),
+            "s_forward_only": round(fwd_s, 4), "peak_mem_gb": round(peak / 1e9, 3), "max_bond": max(bonds),
+            "fd_check": {"angles": LARGE_FD, "h": h, "max_abs_err": float(err.max()),
+                         "max_rel_err": float((err / np.maximum(np.abs(fd), 1e-12)).max()),
+                         "max_abs_grad": float(np.abs(grad).max())}}
+
+
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clock / throttle-reason samples taken while the timed region runs."""
@@ -406,6 +577,12 @@ def run_ours(args) -> None:
     batching = None
     if not args.quick and not args.no_batching:
         batching = batching_leg(dev, 2, rank, max_over_ranks)
+    large = large_leg(dev) if args.large else None
+    gradient = None
+    if not args.quick and not args.no_gradient:
+        from oracle.cpu_baseline import usable_cores
+        cw = usable_cores() if (rank == 0 and world == 1 and not args.no_cpu) else 0
+        gradient = gradient_leg(dev, 3, 2, rank, max_over_ranks, cpu_workers=cw)
 
     if world > 1:
         dist.barrier()
@@ -434,6 +611,8 @@ def run_ours(args) -> None:
         "e2e": e2e,
         "per_update_path": single,
         "batching": batching,
+        "gradient": gradient,
+        "large": large,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -452,6 +631,9 @@ def main():
     ap.add_argument("--mixed-tol", type=float, default=0.0,
                     help="Jacobi off-diagonal tolerance of the mixed form (0 = library default 1e-9)")
     ap.add_argument("--no-batching", action="store_true", help="skip the 256-circuit batching leg")
+    ap.add_argument("--no-gradient", action="store_true", help="skip the ansatz energy-gradient leg")
+    ap.add_argument("--large", action="store_true",
+                    help="add the 1000-qubit XXZ initial-state gradient leg (about a minute)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

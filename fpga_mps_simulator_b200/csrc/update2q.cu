@@ -722,9 +722,10 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
     // other side: Y[rho, col] = sum_r conj(x_j[r]) X0[r, col]
     {
         const double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
-        constexpr int kGroups = NT / 128;
-        const int col = tid & 127, grp = tid >> 7;
-        if (col < C) {
+        constexpr int kCols = NT < 128 ? NT : 128;  // threads per column group
+        constexpr int kGroups = NT / kCols;
+        const int grp = tid / kCols;
+        for (int col = tid - grp * kCols; col < C; col += kCols) {
             for (int base = grp * 8; base < nk; base += 8 * kGroups) {
                 const int nb = min(8, nk - base);
                 const double2 *cpk[8];
@@ -860,18 +861,23 @@ static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb
     p.cut_floor = mixed ? kMixedCutoffFloor : 0.0;
     const size_t smem = mixed ? upd_smem_bytes_mixed(p.wmax, p.rpad, chi_cap) : upd_smem_bytes(p.wmax, p.rpad);
     int rc;
+    // CTA size follows the column count: a slot of C/4 columns holds C/16
+    // quads and a round has at most that many quad tasks per slot pair, so
+    // 128 threads (64 at chi_cap <= 16) keep every warp busy and let two or
+    // more clusters share an SM pair; the tensor-core readout of the mixed
+    // form needs whole 128-thread groups (one warp per TMEM lane quarter).
     if (mixed) {
         if (rpl == 1)
-            rc = launch_rpl<1, kUpdThreads, true>(p, smem, stream);
+            rc = launch_rpl<1, 128, true>(p, smem, stream);
         else if (rpl == 2)
-            rc = launch_rpl<2, kUpdThreads, true>(p, smem, stream);
+            rc = launch_rpl<2, 128, true>(p, smem, stream);
         else
             rc = launch_rpl<4, kUpdThreads, true>(p, smem, stream);
     } else {
         if (rpl == 1)
-            rc = launch_rpl<1, kUpdThreads, false>(p, smem, stream);
+            rc = launch_rpl<1, 64, false>(p, smem, stream);
         else if (rpl == 2)
-            rc = launch_rpl<2, kUpdThreads, false>(p, smem, stream);
+            rc = launch_rpl<2, 128, false>(p, smem, stream);
         else
             rc = launch_rpl<4, kUpdThreads, false>(p, smem, stream);
     }

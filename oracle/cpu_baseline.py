@@ -87,3 +87,44 @@ def run_parallel(n: int, depth: int, chi: int, cutoff: float, workers: int, reps
 
 def make_pool(workers: int):
     return mp.get_context("spawn").Pool(workers)
+
+
+def _grad_worker(args) -> Tuple[int, float]:
+    n, layers, chi, cutoff, seed = args
+    try:
+        from threadpoolctl import threadpool_limits
+        limiter = threadpool_limits(1)
+    except Exception:  # pragma: no cover
+        limiter = None
+    import sys
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if here not in sys.path:
+        sys.path.insert(0, here)
+    from oracle.mps_adjoint import hea_energy_grad, tfim_mpo
+    rng = np.random.default_rng(seed)
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=(layers, n, 2))
+    t0 = time.perf_counter()
+    hea_energy_grad(angles, tfim_mpo(n), chi, cutoff)
+    dt = time.perf_counter() - t0
+    del limiter
+    return 1, dt
+
+
+def run_grad_parallel(n: int, layers: int, chi: int, cutoff: float, workers: int, seed: int = 0,
+                      pool=None) -> Dict[str, float]:
+    """Energy + adjoint gradient of one ansatz parameter vector per worker process
+    (single BLAS thread each); returns aggregate parameter vectors per second."""
+    own = pool is None
+    if own:
+        pool = mp.get_context("spawn").Pool(workers)
+    try:
+        t0 = time.perf_counter()
+        res = pool.map(_grad_worker, [(n, layers, chi, cutoff, seed + w) for w in range(workers)])
+        wall = time.perf_counter() - t0
+    finally:
+        if own:
+            pool.close()
+            pool.join()
+    vecs = sum(r[0] for r in res)
+    return {"vectors": vecs, "wall_s": wall, "vectors_per_s": vecs / wall,
+            "per_worker_s": float(np.mean([r[1] for r in res])), "workers": workers}
