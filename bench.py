@@ -182,9 +182,9 @@ def gradient_leg(dev, steps: int, warmup: int, rank: int, max_over_ranks, cpu_wo
     angles = torch.tensor(hea_angles(GRAD_N, GRAD_LAYERS, GRAD_VEC, SEED + rank), dtype=torch.float64, device=dev)
     out, grads = {}, {}
     flops = None
-    for prec in ("fp64", "mixed"):
+    for prec, ckpt in (("fp64", "auto"), ("mixed", "auto"), ("fp64", True)):
         model = HEAEnergy(GRAD_N, GRAD_LAYERS, GRAD_VEC, chi_max=GRAD_CHI, cutoff=GRAD_CUT, precision=prec,
-                          device=dev, checkpoint=True)
+                          device=dev, checkpoint=ckpt)
         for _ in range(warmup):
             model.energy_and_grad(angles)
         torch.cuda.synchronize()
@@ -198,22 +198,25 @@ def gradient_leg(dev, steps: int, warmup: int, rank: int, max_over_ranks, cpu_wo
         e1.record()
         torch.cuda.synchronize()
         sec = max_over_ranks(e0.elapsed_time(e1) * 1e-3) / steps
-        grads[prec] = (E.clone(), g.clone())
+        key = prec if ckpt == "auto" else f"{prec}_checkpointed"
+        grads[key] = (E.clone(), g.clone())
         if flops is None:
             flops = hea_grad_flops(model, angles)
-        out[prec] = {"s_per_grad_step": round(sec, 5), "grad_steps_per_s": round(1.0 / sec, 4),
-                     "param_vectors_per_s": round(GRAD_VEC / sec, 3),
-                     "launches_per_step": model.engine.launches // steps,
-                     "peak_mem_gb": round((torch.cuda.max_memory_allocated(dev) - base_mem) / 1e9, 3),
-                     "achieved_tflops": round(flops / sec / 1e12, 4)}
+        out[key] = {"s_per_grad_step": round(sec, 5), "grad_steps_per_s": round(1.0 / sec, 4),
+                    "param_vectors_per_s": round(GRAD_VEC / sec, 3),
+                    "recompute": bool(model.engine.checkpointed),
+                    "launches_per_step": model.engine.launches // steps,
+                    "peak_mem_gb": round((torch.cuda.max_memory_allocated(dev) - base_mem) / 1e9, 3),
+                    "achieved_tflops": round(flops / sec / 1e12, 4)}
         del model
         torch.cuda.empty_cache()
     (e64, g64), (emx, gmx) = grads["fp64"], grads["mixed"]
     res = {"workload": (f"{GRAD_VEC} parameter vectors of a {GRAD_N}-qubit hardware-efficient ansatz, "
                         f"{GRAD_LAYERS} layers (RY, RZ every site, CZ brick-wall), chi_max={GRAD_CHI}, "
-                        f"transverse-field Ising energy J=h=1; energy + adjoint gradient per step, "
-                        f"per-layer checkpointing"),
-           "fp64": out["fp64"], "mixed": out["mixed"],
+                        f"transverse-field Ising energy J=h=1; energy + adjoint gradient per step; "
+                        f"tapes kept in HBM (recompute false) or per-layer checkpoints + recomputation"),
+           "fp64": out["fp64"], "mixed": out["mixed"], "fp64_checkpointed": out["fp64_checkpointed"],
+           "checkpointed_equals_taped": bool(torch.equal(grads["fp64"][1], grads["fp64_checkpointed"][1])),
            "mixed_vs_fp64": {"max_abs_energy_diff": float(torch.max(torch.abs(emx - e64))),
                              "max_rel_grad_diff": float(torch.max(torch.abs(gmx - g64)) / torch.max(torch.abs(g64)))},
            "flops_per_step": flops}

@@ -19,7 +19,9 @@ of steps (one ansatz layer, one Trotter step); the backward restores each
 checkpoint in turn, recomputes that group with tapes (bit-identical to the
 forward: same kernels, same inputs) and runs its backward.  With
 ``checkpoint=False`` every step keeps its tape and saved input from the
-forward instead (no recomputation, more memory).
+forward instead (no recomputation, more memory); ``checkpoint="auto"``
+(the default) does that whenever the whole program's tapes fit in half of
+the device memory that is free when the forward starts.
 
 ``HEAEnergy`` is config "differentiation" (RY, RZ on every site, CZ on
 brick-wall pairs, transverse-field Ising energy, many parameter vectors as
@@ -70,7 +72,7 @@ Step = Union[Step1Q, Step2Q]
 class AdjointEngine:
     """Forward with checkpoints and hand-written backward over groups of steps."""
 
-    def __init__(self, batch: MPSBatch, mpo: np.ndarray, checkpoint: bool = True):
+    def __init__(self, batch: MPSBatch, mpo: np.ndarray, checkpoint: Union[bool, str] = "auto"):
         if len(set(batch.ns)) != 1:
             raise ValueError("the energy gradient needs chains of equal length")
         self.b = batch
@@ -79,7 +81,10 @@ class AdjointEngine:
         W = check_mpo(mpo, self.n)
         self.D = W.shape[1]
         self.mpo = torch.from_numpy(W.reshape(-1)).to(batch.device)
+        if checkpoint not in (True, False, "auto"):
+            raise ValueError("checkpoint must be True, False or 'auto'")
         self.checkpoint = checkpoint
+        self.checkpointed = checkpoint is True
         self.cot = torch.zeros_like(batch.sites)
         self.cot_table = batch.make_table(self.cot, batch.bonds)
         self.loss = torch.zeros(batch.nchains, dtype=torch.float64, device=batch.device)
@@ -154,13 +159,30 @@ class AdjointEngine:
         self.launches += 1
 
     # -- whole program ---------------------------------------------------------------
+    def tape_bytes(self, groups: Sequence[Sequence[Step]]) -> int:
+        """Device bytes a forward that keeps every step's tape and input would hold."""
+        b = self.b
+        state = b.sites.numel() * b.sites.element_size() + b.bonds.numel() * 4
+        total = 0
+        for g in groups:
+            for st in g:
+                total += state
+                if isinstance(st, Step2Q):
+                    total += self.lib.mpsb_update2q_tape_bytes(st.pb.npairs, st.chi_cap)
+        return total
+
     def forward(self, groups: Sequence[Sequence[Step]]) -> None:
         """Run the program from the batch's current state, keeping checkpoints (or tapes)."""
         b = self.b
         self.groups = [list(g) for g in groups]
         self.ckpts, self.records = [], []
+        if self.checkpoint == "auto":
+            free, _ = torch.cuda.mem_get_info(b.device)
+            self.checkpointed = self.tape_bytes(self.groups) > free // 2
+        else:
+            self.checkpointed = bool(self.checkpoint)
         for g in self.groups:
-            if self.checkpoint:
+            if self.checkpointed:
                 self.ckpts.append((b.sites.clone(), b.bonds.clone()))
                 for st in g:
                     self._run(st)
@@ -197,7 +219,7 @@ class AdjointEngine:
         grads: Dict[str, torch.Tensor] = {}
         self._bwd_status: List[torch.Tensor] = []
         for gi in range(len(self.groups) - 1, -1, -1):
-            if self.checkpoint:
+            if self.checkpointed:
                 b.sites.copy_(self.ckpts[gi][0])
                 b.bonds.copy_(self.ckpts[gi][1])
                 recs = [self._record(st) for st in self.groups[gi]]
@@ -206,6 +228,8 @@ class AdjointEngine:
             for rec in reversed(recs):
                 self._backward_step(rec, grads)
             del recs
+            if not self.checkpointed:
+                self.records[gi] = None  # release this group's tapes as soon as they are used
         b.sites.copy_(self.final[0])
         b.bonds.copy_(self.final[1])
         if self._bwd_status:
@@ -263,7 +287,7 @@ class HEAEnergy:
 
     def __init__(self, n: int, layers: int, nvec: int, chi_max: int = 32, cutoff: float = 1e-12,
                  precision: str = "fp64", J: float = 1.0, h: float = 1.0,
-                 device: Union[str, torch.device] = "cuda", checkpoint: bool = True):
+                 device: Union[str, torch.device] = "cuda", checkpoint: Union[bool, str] = "auto"):
         self.n, self.layers, self.nvec = int(n), int(layers), int(nvec)
         self.batch = MPSBatch([n] * nvec, chi_max, cutoff, precision=precision, device=device)
         self.device = self.batch.device
@@ -347,7 +371,7 @@ class XXZInitialStateGradient:
 
     def __init__(self, n: int, steps: int, dt: float = 0.05, jxy: float = 1.0, jz: float = 0.5,
                  chi_max: int = 64, cutoff: float = 1e-10, precision: str = "fp64",
-                 device: Union[str, torch.device] = "cuda", checkpoint: bool = True):
+                 device: Union[str, torch.device] = "cuda", checkpoint: Union[bool, str] = "auto"):
         self.n, self.steps = int(n), int(steps)
         self.batch = MPSBatch([n], chi_max, cutoff, precision=precision, device=device)
         self.device = self.batch.device
