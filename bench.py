@@ -41,6 +41,12 @@ WORKLOAD = (f"MPS two-site updates: n={N_SITES} open chain, depth-{DEPTH} Haar b
             f"chi_max={CHI}, cutoff={CUTOFF:g}, each layer's pairs in one launch")
 
 
+# DRAM bytes (read + write) of one saturated-layer launch of the update kernel
+# (49 pairs at chi = 64, mixed form), from one ncu capture of this workload.
+TRAFFIC_PER_LAUNCH = 12.04e6
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, layer 19 of config 2 "
+                  "(profiles/update2q_n100_chi64_mixed_and_fp64.md); algorithmic site reads 12.8 MB")
+
 # ----------------------------------------------------------------- counting
 def update_flops(cl: int, cm: int, cr: int) -> float:
     """Algorithmic flops of one update: contraction 32 cl cm cr, gate 128 cl cr,
@@ -604,7 +610,8 @@ def run_ours(args) -> None:
                    "launches_per_step": 2 * len(layers), "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "flushed between steps (256 MiB write)"},
         "roofline": {"bound": "fp64", "achieved": round(achieved_tf, 4), "peak": round(fp64_peak_tflops, 4),
-                     "unit": "TFLOP/s", "frac": round(achieved_tf / fp64_peak_tflops, 4), "traffic": None,
+                     "unit": "TFLOP/s", "frac": round(achieved_tf / fp64_peak_tflops, 4),
+                     "traffic": TRAFFIC_PER_LAUNCH, "traffic_source": TRAFFIC_SOURCE,
                      "peak_source": "measured: FP64 FMA probe (mpsb_fp64_probe) on this GPU, burst",
                      "kernel": f"update2q kernel ({precision}) + fold_norm_log_kernel",
                      "flops_per_step": flops, "hbm_site_bytes_per_step": hbm,
@@ -621,6 +628,21 @@ def run_ours(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_leg(args) -> None:
+    """One secondary leg alone on GPU 0 (for profiling); prints its JSON object."""
+    import torch
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    ident = lambda x: x  # noqa: E731  (one rank: the max over ranks is the value itself)
+    if args.leg == "gradient":
+        res = gradient_leg(dev, args.steps, args.warmup, 0, ident)
+    elif args.leg == "batching":
+        res = batching_leg(dev, args.steps, 0, ident)
+    else:
+        res = large_leg(dev)
+    print(json.dumps({"leg": args.leg, **res}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -635,6 +657,8 @@ def main():
                     help="Jacobi off-diagonal tolerance of the mixed form (0 = library default 1e-9)")
     ap.add_argument("--no-batching", action="store_true", help="skip the 256-circuit batching leg")
     ap.add_argument("--no-gradient", action="store_true", help="skip the ansatz energy-gradient leg")
+    ap.add_argument("--leg", choices=["all", "gradient", "batching", "large"], default="all",
+                    help="run one secondary leg alone and print its JSON (profiling)")
     ap.add_argument("--large", action="store_true",
                     help="add the 1000-qubit XXZ initial-state gradient leg (about a minute)")
     args = ap.parse_args()
@@ -642,6 +666,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.leg != "all":
+        run_leg(args)
     else:
         run_ours(args)
 
