@@ -26,7 +26,8 @@ EXPORTS = (
     "mpsb_expect_local", "mpsb_fp64_probe", "mpsb_update2q_batch_noalloc", "mpsb_overlap",
     "mpsb_update2q_tape_bytes", "mpsb_update2q_batch_taped", "mpsb_update2q_backward_workspace_bytes",
     "mpsb_update2q_backward_batch", "mpsb_apply1q_backward_batch", "mpsb_mpo_grad_workspace_bytes",
-    "mpsb_mpo_energy_grad",
+    "mpsb_mpo_energy_grad", "mpsb_sample_workspace_bytes", "mpsb_sample", "mpsb_reset_batch",
+    "mpsb_canonicalize_workspace_bytes", "mpsb_canonicalize",
 )
 
 
@@ -84,6 +85,11 @@ def _declare(lib):
         "mpsb_apply1q_backward_batch": (i32, [vp, vp, vp, i32, vp, i32, vp, vp]),
         "mpsb_mpo_grad_workspace_bytes": (sz, [i32, i32, i32, i32]),
         "mpsb_mpo_energy_grad": (i32, [vp, i32, i32, i32, vp, i32, vp, vp, vp, vp, sz, vp]),
+        "mpsb_sample_workspace_bytes": (sz, [i32, i32]),
+        "mpsb_sample": (i32, [vp, i32, i32, i32, vp, i32, vp, vp, sz, vp]),
+        "mpsb_reset_batch": (i32, [vp, vp, i32, i32, vp]),
+        "mpsb_canonicalize_workspace_bytes": (sz, [i32, i32]),
+        "mpsb_canonicalize": (i32, [vp, vp, i32, i32, i32, i32, i32, vp, sz, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -59,6 +59,12 @@ size_t mpo_grad_workspace_bytes(int nchains, int n, int chi_cap, int D);
 int launch_mpo_energy_grad(const mpsb_chain *, int, int, int, const double2 *, int, const double *, double *,
                            const mpsb_chain *, void *, cudaStream_t);
 
+size_t sample_workspace_bytes(int n, int chi_cap);
+int launch_sample(const mpsb_chain *, int, int, int, const double *, int, uint8_t *, void *, cudaStream_t);
+int launch_reset(const mpsb_chain *, const mpsb_site_op *, int, cudaStream_t);
+size_t canon_workspace_bytes(int nchains, int chi_cap);
+int launch_canonicalize(const mpsb_chain *, const int32_t *, int, int, int, int, int, void *, cudaStream_t);
+
 static int expect_ctas() {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -188,6 +194,62 @@ int mpsb_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap, m
     if (rc) return rc;
     return launch_overlap(a, b, n, chi_cap, reinterpret_cast<double2 *>(out), out_log, workspace,
                           reinterpret_cast<cudaStream_t>(stream));
+}
+
+size_t mpsb_sample_workspace_bytes(int n, int chi_cap) {
+    if (n < 1 || chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT) return 0;
+    return sample_workspace_bytes(n, chi_cap);
+}
+
+int mpsb_sample(const mpsb_chain *chains, int chain, int n, int chi_cap, const double *uniforms, int shots,
+                uint8_t *bits, void *workspace, size_t workspace_bytes, mpsb_stream_t stream) {
+    if (!chains || !workspace || (shots > 0 && (!uniforms || !bits)))
+        return set_error(MPSB_EINVAL, "null chains/uniforms/bits/workspace pointer");
+    if (chain < 0 || n < 1 || shots < 0) return set_error(MPSB_EINVAL, "bad chain/n/shots");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    const size_t need = sample_workspace_bytes(n, chi_cap);
+    if (workspace_bytes < need)
+        return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_sample(chains, chain, n, chi_cap, uniforms, shots, bits, workspace,
+                         reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mpsb_reset_batch(const mpsb_chain *chains, const mpsb_site_op *ops, int nops, int chi_cap,
+                     mpsb_stream_t stream) {
+    if (nops < 0) return set_error(MPSB_EINVAL, "nops=%d < 0", nops);
+    if (nops == 0) return MPSB_OK;
+    if (!chains || !ops) return set_error(MPSB_EINVAL, "null chains/ops pointer");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_reset(chains, ops, nops, reinterpret_cast<cudaStream_t>(stream));
+}
+
+size_t mpsb_canonicalize_workspace_bytes(int nchains, int chi_cap) {
+    if (nchains < 0 || chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT) return 0;
+    return canon_workspace_bytes(nchains, chi_cap);
+}
+
+int mpsb_canonicalize(const mpsb_chain *chains, const int32_t *chain_ids, int nchains, int lo, int hi, int direction,
+                      int chi_cap, void *workspace, size_t workspace_bytes, mpsb_stream_t stream) {
+    if (nchains < 0) return set_error(MPSB_EINVAL, "nchains=%d < 0", nchains);
+    if (nchains == 0 || hi < lo) return MPSB_OK;
+    if (!chains || !chain_ids || !workspace) return set_error(MPSB_EINVAL, "null chains/chain_ids/workspace pointer");
+    if (lo < 0) return set_error(MPSB_EINVAL, "lo=%d < 0", lo);
+    if (direction != 0 && direction != 1) return set_error(MPSB_EINVAL, "direction must be 0 (left) or 1 (right)");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    const size_t need = canon_workspace_bytes(nchains, chi_cap);
+    if (workspace_bytes < need)
+        return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
+    int rc = check_device();
+    if (rc) return rc;
+    return launch_canonicalize(chains, chain_ids, nchains, lo, hi, direction, chi_cap, workspace,
+                               reinterpret_cast<cudaStream_t>(stream));
 }
 
 size_t mpsb_update2q_tape_bytes(int npairs, int chi_cap) {

@@ -338,6 +338,62 @@ class MPSBatch:
         _lib.check(rc, "mpsb_amplitude")
         return (out.cpu().numpy(), la.cpu().numpy()) if with_log else out.cpu().numpy()
 
+    def sample_bits(self, c: int, uniforms: np.ndarray) -> np.ndarray:
+        """Shots of chain c as a (shots, n) uint8 array (column i = qubit i).
+
+        ``uniforms`` (shots, n) in [0, 1) drive the draws in (shot, site)
+        order, one per draw, as the reference's per-site rng.choice does.
+        """
+        n = self.ns[c]
+        u = np.ascontiguousarray(np.asarray(uniforms, np.float64).reshape(-1, n))
+        shots = u.shape[0]
+        if shots == 0:
+            return np.zeros((0, n), np.uint8)
+        ut = torch.from_numpy(u).to(self.device)
+        bits = torch.empty(shots, n, dtype=torch.uint8, device=self.device)
+        need = self._lib.mpsb_sample_workspace_bytes(n, self.chi_cap)
+        ws = self._ews.get(need)
+        rc = self._lib.mpsb_sample(self.table.data_ptr(), c, n, self.chi_cap, ut.data_ptr(), shots, bits.data_ptr(),
+                                   ws.data_ptr(), ws.numel(), self._stream())
+        _lib.check(rc, "mpsb_sample")
+        return bits.cpu().numpy()
+
+    def reset_many(self, chain_idx, sites) -> None:
+        """Reset of fpga_mps_simulator.py:530-552 on distinct (chain, site) pairs, one launch."""
+        chain_idx = np.asarray(chain_idx, np.int32).reshape(-1)
+        sites = np.asarray(sites, np.int32).reshape(-1)
+        if len(sites) == 0:
+            return
+        if np.any(sites < 0) or np.any(sites >= np.asarray(self.ns)[chain_idx]):
+            raise ValueError("site out of range")
+        key = chain_idx.astype(np.int64) * (1 << 32) + sites
+        if len(np.unique(key)) != len(key):
+            raise ValueError("reset sites of one launch must be distinct")
+        ops = np.stack([chain_idx, sites, np.zeros_like(sites), np.zeros_like(sites)], 1)
+        ops_t = torch.from_numpy(np.ascontiguousarray(ops)).to(self.device)
+        rc = self._lib.mpsb_reset_batch(self.table.data_ptr(), ops_t.data_ptr(), len(sites), self.chi_cap,
+                                        self._stream())
+        _lib.check(rc, "mpsb_reset_batch")
+
+    def canonicalize(self, chains: Sequence[int], lo: int, hi: int, direction: str = "left") -> None:
+        """QR sweeps on the listed chains: "left" = left_normalize_site(i) for
+        i = lo..hi, "right" = right_normalize_site(i) for i = hi..lo
+        (mps_core.py:221-252), one launch."""
+        chains = [int(c) for c in chains]
+        if not chains or hi < lo:
+            return
+        if lo < 0 or any(hi >= self.ns[c] for c in chains):
+            raise ValueError("canonicalisation range outside a chain")
+        if direction not in ("left", "right"):
+            raise ValueError("direction must be 'left' or 'right'")
+        ids = torch.tensor(chains, dtype=torch.int32, device=self.device)
+        need = self._lib.mpsb_canonicalize_workspace_bytes(len(chains), self.chi_cap)
+        ws = self._ews.get(need)
+        rc = self._lib.mpsb_canonicalize(self.table.data_ptr(), ids.data_ptr(), len(chains), int(lo), int(hi),
+                                         0 if direction == "left" else 1, self.chi_cap, ws.data_ptr(), ws.numel(),
+                                         self._stream())
+        _lib.check(rc, "mpsb_canonicalize")
+
     def expect_terms(self, terms: Sequence[Tuple[int, np.ndarray, Optional[np.ndarray]]],
                      chains: Optional[Sequence[int]] = None) -> np.ndarray:
         """Normalised <O> for terms (site, O_site, O_next or None) on chains 0..nchains-1.
@@ -541,6 +597,98 @@ class MPSState:
             bits = [int(ch) for ch in reversed(bits)]
         self.check_status()
         return complex(self._b.amplitudes(0, np.asarray(bits)[None, :])[0])
+
+    # -- canonical forms (mps_core.py:219-261) ----------------------------------
+    def left_normalize_site(self, i: int) -> None:
+        """QR of site i; Q stays, R is absorbed into site i+1 (mps_core.py:221-235)."""
+        self._b.canonicalize([0], i, i, "left")
+
+    def right_normalize_site(self, i: int) -> None:
+        """LQ of site i; L is absorbed into site i-1 (mps_core.py:237-252)."""
+        self._b.canonicalize([0], i, i, "right")
+
+    def left_canonicalize(self) -> None:
+        """left_normalize_site(i) for i = 0 .. n-2 (mps_core.py:254-257), one launch."""
+        self._b.canonicalize([0], 0, self.n - 2, "left")
+
+    def right_canonicalize(self) -> None:
+        """right_normalize_site(i) for i = n-1 .. 1 (mps_core.py:259-261), one launch."""
+        self._b.canonicalize([0], 1, self.n - 1, "right")
+
+    def schmidt_values(self, bond: int) -> np.ndarray:
+        """Normalised Schmidt coefficients across the cut between sites bond and bond+1.
+
+        The reference reads spectra off its non-canonical gauge
+        (``entanglement_entropy`` assumes a mixed-canonical state,
+        ``bond_spectrum`` returns the singular values of an isometry, i.e.
+        ones); this brings a copy into mixed-canonical form around the cut
+        (sites left of it left-normalised, right of it right-normalised) and
+        takes the spectrum of the two-site theta there with the fused
+        update kernel.  The state itself is not changed.
+        """
+        if not 0 <= bond < self.n - 1:
+            raise ValueError(f"bond {bond} out of range [0, {self.n - 2}]")
+        self.check_status()
+        m = self.copy()
+        m._b.precision = "fp64"
+        if bond >= 1:
+            m._b.canonicalize([0], 0, bond - 1, "left")
+        if bond + 2 <= self.n - 1:
+            m._b.canonicalize([0], bond + 2, self.n - 1, "right")
+        pb = m._b.apply_layer([0], [bond], np.eye(4, dtype=np.complex128)[None], record_spectra=True)
+        s = pb.spectra[0].cpu().numpy()
+        s = s[s > 0.0]
+        s = s / np.linalg.norm(s)
+        return s[s > 1e-15]
+
+    def entanglement_entropy(self, bond: int) -> float:
+        """von Neumann entropy -sum p log p, p = Schmidt coefficients squared, at the cut after site ``bond``
+        (the quantity of mps_core.py:465-483, exact in any gauge)."""
+        p = self.schmidt_values(bond) ** 2
+        return -float(np.sum(p * np.log(np.maximum(p, 1e-300))))
+
+    # -- measurement (mps_core.py:354-429) ------------------------------------
+    def sample(self, num_shots: int = 1, measured_qubits: Optional[Sequence[int]] = None,
+               rng: Optional[np.random.Generator] = None) -> List[str]:
+        """Shots as bitstrings (msb = qubit n-1), as MPSState.sample (mps_core.py:371-419).
+
+        The draws use one uniform of ``rng`` per (shot, site), in the order the
+        reference's per-site ``rng.choice(2, p=...)`` consumes them, so the
+        same seeded generator gives the reference's shots.  For a qubit subset
+        the bitstring is bits[n-1-q] over the qubits in decreasing order, as
+        the reference builds it (mps_core.py:414-416).
+        """
+        if rng is None:
+            rng = np.random.default_rng()
+        if num_shots < 0:
+            raise ValueError("num_shots must be >= 0")
+        self.check_status()
+        u = rng.random((num_shots, self.n))
+        bits = self._b.sample_bits(0, u)
+        out = []
+        subset = measured_qubits is not None and set(measured_qubits) != set(range(self.n))
+        ms = sorted(measured_qubits, reverse=True) if subset else None
+        chars = np.where(bits == 1, "1", "0")
+        for row in chars:
+            if subset:
+                out.append("".join(row[self.n - 1 - q] for q in ms))
+            else:
+                out.append("".join(row[::-1]))
+        return out
+
+    def get_counts(self, num_shots: int, measured_qubits: Optional[Sequence[int]] = None,
+                   rng: Optional[np.random.Generator] = None) -> Dict[str, int]:
+        """Sample and count (mps_core.py:421-429)."""
+        counts: Dict[str, int] = {}
+        for s in self.sample(num_shots, measured_qubits, rng):
+            counts[s] = counts.get(s, 0) + 1
+        return counts
+
+    def reset(self, site: int) -> None:
+        """Site reset of the reference's execution engine (fpga_mps_simulator.py:530-552)."""
+        if not 0 <= site < self.n:
+            raise ValueError("site out of range")
+        self._b.reset_many([0], [site])
 
     def expectation(self, op: Union[str, Dict[int, np.ndarray]]) -> float:
         """Normalised <psi|O|psi>/<psi|psi> for a local operator.

@@ -189,6 +189,45 @@ MPSB_API int mpsb_expect_local(const mpsb_chain *chains, int nchains, int n, int
 MPSB_API int mpsb_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap, mpsb_c128 *out,
                           double *out_log, void *workspace, size_t workspace_bytes, mpsb_stream_t stream);
 
+/* ---------------------------------------------------------------- measurement */
+
+/* Bytes of device workspace mpsb_sample needs (right environments). */
+MPSB_API size_t mpsb_sample_workspace_bytes(int n, int chi_cap);
+
+/* Conditional shot sampling of chain `chain` (n sites), replacing
+ * MPSState.sample (mps_core.py:354-419): right environments, then per shot
+ * a left-to-right sweep drawing each site's outcome.  uniforms: device,
+ * shots x n doubles in [0, 1), one per (shot, site) in that order; site i of
+ * shot k is 1 exactly when uniforms[k*n+i] >= p0 / (p0 + p1), the rule by
+ * which numpy's Generator.choice(2, p) (the reference's draw) maps its one
+ * uniform to an outcome, so the uniforms of the same seeded generator give
+ * the reference's shots.  bits: device, shots x n bytes (byte i = site i). */
+MPSB_API int mpsb_sample(const mpsb_chain *chains, int chain, int n, int chi_cap, const double *uniforms,
+                         int shots, uint8_t *bits, void *workspace, size_t workspace_bytes,
+                         mpsb_stream_t stream);
+
+/* Site reset of _run_circuit_fpga (fpga_mps_simulator.py:530-552) for a batch
+ * of distinct sites: zero the sigma = 1 half, divide by the remaining
+ * Frobenius norm when it exceeds 1e-15, else set the tensor to zeros with a
+ * 1 at [0, 0, 0].  ops: device (the gate field is ignored). */
+MPSB_API int mpsb_reset_batch(const mpsb_chain *chains, const mpsb_site_op *ops, int nops, int chi_cap,
+                              mpsb_stream_t stream);
+
+/* Bytes of device workspace mpsb_canonicalize needs for nchains chains. */
+MPSB_API size_t mpsb_canonicalize_workspace_bytes(int nchains, int chi_cap);
+
+/* Canonical-form sweeps on chains chain_ids[0 .. nchains-1] (device array),
+ * one CTA per chain.  direction 0: left_normalize_site(i) for i = lo .. hi
+ * (mps_core.py:221-235: QR of site i as (2 chi_l) x chi_r, Q stays, R is
+ * absorbed into site i+1); direction 1: right_normalize_site(i) for
+ * i = hi .. lo (mps_core.py:237-252: LQ, L absorbed into site i-1).  The QR
+ * follows LAPACK zgeqr2 / zung2r (the routines numpy.linalg.qr calls), so on
+ * the same input the sites agree with the reference's to rounding.  Bonds are
+ * updated on the device (k = min(rows, cols) of each QR). */
+MPSB_API int mpsb_canonicalize(const mpsb_chain *chains, const int32_t *chain_ids, int nchains, int lo, int hi,
+                               int direction, int chi_cap, void *workspace, size_t workspace_bytes,
+                               mpsb_stream_t stream);
+
 /* ---------------------------------------------------------------- adjoint
  * No reference counterpart: the reference engine has no gradients.  These
  * entries differentiate exactly what mpsb_update2q_batch and

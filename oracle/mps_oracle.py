@@ -151,6 +151,56 @@ class OracleMPS:
             t[0, 0, 0] = 1.0
         self.sites[site] = t
 
+    # -- canonical forms (mps_core.py:219-261) ---------------------------------
+    def left_normalize_site(self, i: int) -> None:
+        """QR of site i as (chi_l*2) x chi_r; Q stays, R is absorbed into site i+1."""
+        a = self.sites[i]
+        cl, d, cr = a.shape
+        q, r = np.linalg.qr(a.reshape(cl * d, cr))
+        self.sites[i] = q.reshape(cl, d, q.shape[1])
+        if i + 1 < self.n:
+            self.sites[i + 1] = np.tensordot(r, self.sites[i + 1], axes=([1], [0]))
+
+    def right_normalize_site(self, i: int) -> None:
+        """LQ of site i as chi_l x (2*chi_r) (QR of its conjugate transpose); L absorbed into site i-1."""
+        a = self.sites[i]
+        cl, d, cr = a.shape
+        q, r = np.linalg.qr(a.reshape(cl, d * cr).T.conj())
+        lmat = r.T.conj()
+        b = q.T.conj()
+        self.sites[i] = b.reshape(b.shape[0], d, cr)
+        if i - 1 >= 0:
+            self.sites[i - 1] = np.tensordot(self.sites[i - 1], lmat, axes=([2], [0]))
+
+    def left_canonicalize(self) -> None:
+        for i in range(self.n - 1):
+            self.left_normalize_site(i)
+
+    def right_canonicalize(self) -> None:
+        for i in range(self.n - 1, 0, -1):
+            self.right_normalize_site(i)
+
+    def entanglement_entropy(self, bond: int) -> float:
+        """mps_core.py:465-483: SVD of the contracted left block (sites 0..bond), S > 1e-15."""
+        if bond < 0 or bond >= self.n - 1:
+            raise ValueError(f"bond {bond} out of range [0, {self.n - 2}]")
+        a = self.sites[0][0, :, :]
+        for i in range(1, bond + 1):
+            a = np.tensordot(a, self.sites[i], axes=([1], [0])).reshape(-1, self.sites[i].shape[2])
+        s = sla.svd(a, full_matrices=False, compute_uv=False)
+        s = s[s > 1e-15]
+        p = s ** 2
+        p = p / p.sum()
+        return -float(np.sum(p * np.log(np.maximum(p, 1e-300))))
+
+    def bond_spectrum(self, bond: int) -> np.ndarray:
+        """mps_core.py:485-494: left-normalise sites 0..bond of a copy, SVD of site `bond`."""
+        m = self.copy()
+        for i in range(bond + 1):
+            m.left_normalize_site(i)
+        a = m.sites[bond]
+        return sla.svd(a.reshape(-1, a.shape[2]), full_matrices=False, compute_uv=False)
+
     # -- read-out -------------------------------------------------------------
     def statevector(self) -> np.ndarray:
         """Dense amplitudes in Qiskit order, including exp(norm_log) (mps_core.py:433-461)."""
@@ -238,14 +288,27 @@ class OracleMPS:
         out[self.n] = np.ones((1, 1), np.complex128)
         for k in range(self.n - 1, -1, -1):
             a = self.sites[k]
-            e = np.einsum("isb,jsb->ij", np.einsum("isc,bc->isb", a, out[k + 1]), a.conj())
+            # R_new[i, j] = sum_{s,b,c} A[i,s,b] R[b,c] conj(A[j,s,c])  (mps_core.py:364)
+            e = np.einsum("isc,jsc->ij", np.einsum("isb,bc->isc", a, out[k + 1]), a.conj())
             tr = float(np.real(np.trace(e)))
             if tr > 1e-300:
                 e = e / tr
             out[k] = e
         return out
 
-    def sample(self, num_shots: int, rng: np.random.Generator) -> List[str]:
+    def sample(self, num_shots: int = 1, measured_qubits: Optional[Sequence[int]] = None,
+               rng: Optional[np.random.Generator] = None) -> List[str]:
+        """Sequential conditional sampling, mps_core.py:371-419 (one rng.choice per site and shot).
+
+        A second positional argument that is a Generator is taken as ``rng``
+        (the reference's signature is (num_shots, measured_qubits, rng)).  For a
+        qubit subset the bitstring is built as bits[n-1-q] over the qubits in
+        decreasing order, exactly as mps_core.py:414-416 does.
+        """
+        if isinstance(measured_qubits, np.random.Generator):
+            measured_qubits, rng = None, measured_qubits
+        if rng is None:
+            rng = np.random.default_rng()
         envs = self.right_environments()
         shots = []
         for _ in range(num_shots):
@@ -266,7 +329,11 @@ class OracleMPS:
                 nv = float(np.linalg.norm(v))
                 if nv > 1e-15:
                     v = v / nv
-            shots.append("".join(str(b) for b in reversed(bits)))
+            bs = "".join(str(b) for b in reversed(bits))
+            if measured_qubits is not None and set(measured_qubits) != set(range(self.n)):
+                ms = sorted(measured_qubits, reverse=True)
+                bs = "".join(str(bits[self.n - 1 - q]) for q in ms)
+            shots.append(bs)
         return shots
 
 

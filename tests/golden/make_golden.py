@@ -3,7 +3,7 @@
 Run from the repository root in a container where the reference checkout is
 mounted (read-only) at /root/reference:
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py [/path/to/reference] [run_NAME ...]
 
 It imports the reference's ``mps_core.py`` unchanged, drives it through its own
 public methods (``apply_1q``, ``apply_2q``, ``_apply_adjacent_2q``,
@@ -26,7 +26,8 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+_ARGS = [a for a in sys.argv[1:] if not a.startswith("--")]
+REF = _ARGS[0] if _ARGS and not _ARGS[0].startswith("run_") and os.path.isdir(_ARGS[0]) else "/root/reference"
 sys.path.insert(0, REF)
 import mps_core  # noqa: E402  (the reference module, unchanged)
 
@@ -196,10 +197,66 @@ def run_xxz():
     print("xxz max bond", st.max_bond(), "norm_log", st.norm_log)
 
 
+def pack_sites(sites):
+    shapes = np.array([t.shape for t in sites], np.int32)
+    flat = np.concatenate([t.reshape(-1) for t in sites])
+    return shapes, flat
+
+
+def run_measure():
+    """Shots of MPSState.sample / get_counts and the canonical-form helpers
+    (left/right_normalize_site sweeps, entanglement_entropy, bond_spectrum)."""
+    n, depth, chi, cutoff, seed = 16, 10, 16, 1e-12, 1234
+    st = mps_core.MPSState(n, chi, cutoff)
+    for i, g in brick(n, depth, seed):
+        st._apply_adjacent_2q(i, g)
+    shots = st.sample(400, rng=np.random.default_rng(11))
+    sub_q = [0, 3, 7, 12]
+    sub = st.sample(200, measured_qubits=sub_q, rng=np.random.default_rng(12))
+    counts = st.get_counts(300, rng=np.random.default_rng(13))
+    # canonical forms of a random, non-canonical chain
+    rng = np.random.default_rng(21)
+    bonds = [1, 2, 4, 8, 6, 5, 3, 2, 1]
+    m = len(bonds) - 1
+    sites = [(rng.standard_normal((bonds[k], 2, bonds[k + 1]))
+              + 1j * rng.standard_normal((bonds[k], 2, bonds[k + 1]))) for k in range(m)]
+    ref = mps_core.MPSState(m, 64, 1e-12)
+    ref.sites = [t.copy() for t in sites]
+    ent = np.array([ref.entanglement_entropy(b) for b in range(m - 1)])
+    spec = [ref.bond_spectrum(b) for b in range(m - 1)]
+    left = ref.copy()
+    left.left_canonicalize()
+    right = ref.copy()
+    right.right_canonicalize()
+    in_shapes, in_flat = pack_sites(sites)
+    l_shapes, l_flat = pack_sites(left.sites)
+    r_shapes, r_flat = pack_sites(right.sites)
+    sp_len = np.array([len(x) for x in spec], np.int32)
+    sp = np.zeros((len(spec), sp_len.max()))
+    for k, x in enumerate(spec):
+        sp[k, :len(x)] = x
+    np.savez_compressed(os.path.join(HERE, "measure.npz"), n=n, depth=depth, chi_max=chi, cutoff=cutoff,
+                        seed=seed, shots=np.array(shots), sub_qubits=np.array(sub_q, np.int32),
+                        sub_shots=np.array(sub), count_keys=np.array(sorted(counts)),
+                        count_vals=np.array([counts[k] for k in sorted(counts)], np.int64),
+                        canon_in_shapes=in_shapes, canon_in=in_flat, left_shapes=l_shapes, left=l_flat,
+                        right_shapes=r_shapes, right=r_flat, entropy=ent, bond_spectrum=sp,
+                        bond_spectrum_len=sp_len)
+    print("measure: shots", len(shots), "distinct", len(set(shots)))
+
+
+RUNS = {
+    "run_gate_tables": run_gate_tables,
+    "run_diag_circuits": run_diag_circuits,
+    "run_brick_n16": lambda: run_brick("brick_n16_d10_chi16", 16, 10, 16, 1e-12, 1234, full_sv=True),
+    "run_brick_n40": lambda: run_brick("brick_n40_d16_chi32", 40, 16, 32, 1e-10, 77),
+    "run_brick_n20": lambda: run_brick("brick_n20_d12_chi64", 20, 12, 64, 1e-10, 4242),
+    "run_xxz": run_xxz,
+    "run_measure": run_measure,
+}
+
 if __name__ == "__main__":
-    run_gate_tables()
-    run_diag_circuits()
-    run_brick("brick_n16_d10_chi16", 16, 10, 16, 1e-12, 1234, full_sv=True)
-    run_brick("brick_n40_d16_chi32", 40, 16, 32, 1e-10, 77)
-    run_brick("brick_n20_d12_chi64", 20, 12, 64, 1e-10, 4242)
-    run_xxz()
+    only = [a for a in sys.argv[1:] if a.startswith("run_")]
+    for name, fn in RUNS.items():
+        if not only or name in only:
+            fn()
