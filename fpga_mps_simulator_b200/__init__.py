@@ -3,7 +3,8 @@ from .gates import (GATE_MATRICES, SINGLE_QUBIT_GATES, TWO_QUBIT_GATES, gate_1q,
                     swap_route)
 
 __all__ = ["GATE_MATRICES", "SINGLE_QUBIT_GATES", "TWO_QUBIT_GATES", "gate_1q", "gate_2q", "permute_2q",
-           "swap_route", "MPSState", "MPSBatch"]
+           "swap_route", "MPSState", "MPSBatch", "MPSSimulator", "MPSResult", "Circuit", "HEAEnergy",
+           "HEAEnergyFunction"]
 
 
 def __getattr__(name):
@@ -11,4 +12,10 @@ def __getattr__(name):
     if name in ("MPSState", "MPSBatch", "PairBatch"):
         from . import mps
         return getattr(mps, name)
+    if name in ("MPSSimulator", "MPSResult", "Circuit"):
+        from . import compiler
+        return getattr(compiler, name)
+    if name in ("HEAEnergy", "HEAEnergyFunction", "XXZInitialStateGradient"):
+        from . import adjoint
+        return getattr(adjoint, name)
     raise AttributeError(name)

@@ -245,6 +245,109 @@ def run_measure():
     print("measure: shots", len(shots), "distinct", len(set(shots)))
 
 
+class _Q:
+    def __init__(self, i):
+        self.index = i
+
+
+class _Inst:
+    def __init__(self, name, qubits, params):
+        self.operation = type("Op", (), {"name": name, "params": list(params)})()
+        self.qubits = qubits
+
+
+class DuckCircuit:
+    """The attribute shape of qiskit's QuantumCircuit that compile_circuit reads."""
+
+    def __init__(self, n):
+        self.num_qubits = n
+        self.qubits = [_Q(i) for i in range(n)]
+        self.data = []
+
+    def find_bit(self, q):
+        return type("Loc", (), {"index": q.index})()
+
+    def add(self, name, qs, params=()):
+        self.data.append(_Inst(name, [self.qubits[q] for q in qs], params))
+
+
+def random_instructions(seed):
+    """Seeded random instruction list (name, qubits, params) over 3..9 qubits."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(3, 10))
+    out = []
+    for _ in range(int(rng.integers(10, 40))):
+        k = int(rng.integers(0, 7))
+        if k < 2:
+            out.append((str(rng.choice(["h", "x", "t", "sdg", "sx", "y"])), [int(rng.integers(n))], []))
+        elif k == 2:
+            out.append(("u", [int(rng.integers(n))], [float(v) for v in rng.uniform(-3, 3, 3)]))
+        elif k in (3, 4):
+            a, b = rng.choice(n, 2, replace=False)
+            nm = str(rng.choice(["cx", "cz", "rzz", "swap", "cp", "ecr", "iswap", "rxx"]))
+            out.append((nm, [int(a), int(b)], [0.37] if nm in ("rzz", "cp", "rxx") else []))
+        elif k == 5:
+            a, b, t = rng.choice(n, 3, replace=False)
+            out.append(("ccx", [int(a), int(b), int(t)], []))
+        else:
+            out.append(("measure" if rng.random() < 0.6 else "reset", [int(rng.integers(n))], []))
+    return n, out
+
+
+def run_compiler():
+    """Reference compile_circuit on seeded random circuits, then the gate list
+    executed by the reference engine (MPSState for the gates, the reset branch of
+    _run_circuit_fpga restated, get_counts with default_rng(seed + index))."""
+    import fpga_mps_simulator as fms  # the reference execution engine module, unchanged
+    out = {}
+    base_seed, shots = 100, 256
+    for idx in range(12):
+        n, ins = random_instructions(1000 + idx)
+        c = DuckCircuit(n)
+        for nm, qs, ps in ins:
+            c.add(nm, qs, ps)
+        gl, meas = fms.compile_circuit(c, n)
+        st = mps_core.MPSState(n, 64, 1e-12)
+        for g in gl:
+            if g["type"] == "1q":
+                st.apply_1q(g["sites"][0], g["gate_mat"])
+            elif g["type"] == "2q":
+                st._apply_adjacent_2q(g["sites"][0], g["gate_mat"])
+            else:
+                s = g["sites"][0]
+                t = st.sites[s].copy()
+                t[:, 1, :] = 0.0
+                nm = np.linalg.norm(t)
+                if nm > 1e-15:
+                    t /= nm
+                else:
+                    t = np.zeros_like(t)
+                    t[0, 0, 0] = 1.0
+                st.sites[s] = t
+        counts = st.get_counts(shots, meas, np.random.default_rng(base_seed + idx))
+        p = f"c{idx}_"
+        out[p + "n"] = n
+        out[p + "ins_names"] = np.array([i[0] for i in ins])
+        out[p + "ins_qubits"] = np.array([i[1] + [-1] * (3 - len(i[1])) for i in ins], np.int32)
+        out[p + "ins_params"] = np.array([i[2] + [0.0] * (3 - len(i[2])) for i in ins])
+        out[p + "ins_nparams"] = np.array([len(i[2]) for i in ins], np.int32)
+        out[p + "gl_type"] = np.array([g["type"] for g in gl])
+        out[p + "gl_name"] = np.array([g["gate_name"] for g in gl])
+        out[p + "gl_sites"] = np.array([g["sites"] + [-1] * (2 - len(g["sites"])) for g in gl], np.int32)
+        out[p + "gl_mat"] = np.stack([np.zeros(16, complex) if g["gate_mat"] is None
+                                      else np.pad(np.asarray(g["gate_mat"]).reshape(-1), (0, 16 - g["gate_mat"].size))
+                                      for g in gl])
+        out[p + "measured"] = np.array(meas, np.int32)
+        out[p + "sv"] = st.get_statevector()
+        out[p + "count_keys"] = np.array(sorted(counts))
+        out[p + "count_vals"] = np.array([counts[k] for k in sorted(counts)], np.int64)
+    out["count"] = 12
+    out["shots"] = shots
+    out["seed"] = base_seed
+    np.savez_compressed(os.path.join(HERE, "compiler.npz"), **out)
+    print("compiler: 12 circuits")
+
+
 RUNS = {
     "run_gate_tables": run_gate_tables,
     "run_diag_circuits": run_diag_circuits,
@@ -253,6 +356,7 @@ RUNS = {
     "run_brick_n20": lambda: run_brick("brick_n20_d12_chi64", 20, 12, 64, 1e-10, 4242),
     "run_xxz": run_xxz,
     "run_measure": run_measure,
+    "run_compiler": run_compiler,
 }
 
 if __name__ == "__main__":
