@@ -415,18 +415,15 @@ def run_reference(args) -> None:
 # ----------------------------------------------------------------- GPU side
 def run_ours(args) -> None:
     import torch
-    import torch.distributed as dist
     from fpga_mps_simulator_b200 import MPSBatch, MPSState, _lib
     from fpga_mps_simulator_b200.circuits import brickwall_layers
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from fpga_mps_simulator_b200.replicas import Replicas
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    reps = Replicas("nccl", dev, timeout_s=300)
+    world, rank = reps.world, reps.rank
     lib = _lib.load()
     precision = args.precision
 
@@ -436,7 +433,7 @@ def run_ours(args) -> None:
         from oracle.cpu_baseline import usable_cores
         cpu = cpu_baseline_sample(usable_cores())
 
-    layers = brickwall_layers(N_SITES, DEPTH, SEED + rank)
+    layers = brickwall_layers(N_SITES, DEPTH, reps.seed(SEED))
     n_upd = sum(len(L.sites) for L in layers)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
@@ -447,16 +444,8 @@ def run_ours(args) -> None:
         b.norm_logs.zero_()
         b.status_acc.zero_()
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = reps.barrier
+    max_over_ranks = reps.max
 
     # ---- FP64 peak probe (the roofline denominator for the FP64-bound kernel)
     props = torch.cuda.get_device_properties(dev)
@@ -593,9 +582,7 @@ def run_ours(args) -> None:
         cw = usable_cores() if (rank == 0 and world == 1 and not args.no_cpu) else 0
         gradient = gradient_leg(dev, 3, 2, rank, max_over_ranks, cpu_workers=cw)
 
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    reps.close()
     if rank != 0:
         return
     line = {
