@@ -34,6 +34,12 @@ namespace mpsb {
 // 256 threads per CTA: eight warps, one column-quad task per warp and round
 // at chi = 64 (a slot holds up to eight quads), up to 255 registers each.
 constexpr int kUpdThreads = 256;
+#ifndef MPSB_RPL2_MIN_BLOCKS
+#define MPSB_RPL2_MIN_BLOCKS 3
+#endif
+#ifndef MPSB_RPL1_MIN_BLOCKS
+#define MPSB_RPL1_MIN_BLOCKS 6
+#endif
 constexpr double kMixedCutoffFloor = 1e-6;
 
 struct Upd2Params {
@@ -449,8 +455,19 @@ __device__ void exchange_slots(cg::cluster_group &cluster, const Slots &S, doubl
     __syncthreads();
 }
 
+// Resident CTAs per SM the register allocation is held to (more co-resident
+// clusters hide more FP64 latency): at chi_cap <= 32 (RPL = 2, 128 threads,
+// ~51 KB shared) three (168 registers: 7 % faster than two at 230); at
+// chi_cap <= 16 (RPL = 1, ~13 KB shared) MPSB_RPL1_MIN_BLOCKS.
+template <int RPL, int NT>
+struct UpdMinBlocks {
+    static constexpr int value = RPL == 2 ? MPSB_RPL2_MIN_BLOCKS
+                                 : RPL == 1 ? (NT == 64 ? MPSB_RPL1_MIN_BLOCKS : MPSB_RPL1_MIN_BLOCKS / 2)
+                                            : 1;
+};
+
 template <int RPL, int NT, bool MIXED>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, 1)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RPL, NT>::value))
     update2q_fp64_kernel(const Upd2Params p) {
     constexpr int kUpdThreads = NT;
     constexpr int kUpdWarps = NT / 32;
@@ -856,6 +873,10 @@ static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb
     p.wmax = (((2 * chi_cap) + 15) & ~15) / 4;
     p.tol2 = tol * tol;
     p.max_sweeps = max_sweeps;
+    // At chi_cap <= 16 a 128-row tensor-core tile is mostly padding and the
+    // FP64 contraction is both exact and faster (measured: 37 vs 55 ms per
+    // 64-vector ansatz forward), so the mixed form uses it there.
+    if (mixed && rpl == 1) mixed = false;
     // 3xTF32 theta carries relative errors near 1e-7, so singular values below
     // ~1e-6 S[0] are rounding noise: the mixed form never keeps them
     p.cut_floor = mixed ? kMixedCutoffFloor : 0.0;

@@ -79,7 +79,9 @@ enum mpsb_precision {
     MPSB_FP64 = 0,        /* complex128 end to end (the drop-in form)                    */
     MPSB_MIXED_TF32X3 = 1 /* theta by 3xTF32 complex-3M tensor-core GEMMs (tcgen05), FP64
                              Jacobi SVD; singular values below 1e-6 S[0] (theta's rounding
-                             floor) are never kept, whatever the cutoff                 */
+                             floor) are never kept, whatever the cutoff.  At chi_cap <= 16
+                             the contraction runs in FP64 (exact, no floor): the tensor-core
+                             tile would be mostly padding                               */
 };
 
 enum mpsb_status_bits {
