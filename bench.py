@@ -243,14 +243,23 @@ def gradient_leg(dev, steps: int, warmup: int, rank: int, max_over_ranks, cpu_wo
                                      "chi=32-truncated state itself differs (state infidelity ~1e-6)"},
            "flops_per_step": flops}
     if cpu_workers:
-        from oracle.cpu_baseline import make_pool, run_grad_parallel
+        from oracle.cpu_baseline import make_pool, run_forward_parallel, run_grad_parallel
         pool = make_pool(cpu_workers)
         try:
             run_grad_parallel(8, 1, 4, GRAD_CUT, cpu_workers, pool=pool)
             r = run_grad_parallel(GRAD_N, GRAD_LAYERS, GRAD_CHI, GRAD_CUT, cpu_workers, seed=SEED, pool=pool)
+            f = run_forward_parallel(GRAD_N, GRAD_LAYERS, GRAD_CHI, GRAD_CUT, cpu_workers, seed=SEED, pool=pool)
         finally:
             pool.close()
             pool.join()
+        n_params = GRAD_LAYERS * GRAD_N * 2
+        ps_step = (2 * n_params + 1) * f["s_per_eval"] * GRAD_VEC / cpu_workers
+        res["cpu_parameter_shift"] = {
+            "value": round(ps_step, 1), "unit": "s/grad step", "cores": cpu_workers, "kind": "port",
+            "sample": (f"one energy evaluation per process ({f['s_per_eval']:.2f} s, the reference's update "
+                       f"semantics), extrapolated to 2P+1 = {2 * n_params + 1} evaluations per vector x "
+                       f"{GRAD_VEC} vectors over {cpu_workers} processes: the parameter-shift gradient the "
+                       "reference engine would need")}
         res["cpu_baseline"] = {"value": round(GRAD_VEC / r["vectors_per_s"], 3), "unit": "s/grad step",
                                "cores": cpu_workers, "kind": "port",
                                "sample": (f"{cpu_workers} single-BLAS-thread processes, one parameter vector each "
@@ -395,7 +404,7 @@ class ClockSampler:
 
 # ----------------------------------------------------------------- CPU side
 def cpu_baseline_sample(workers: int):
-    from oracle.cpu_baseline import make_pool, run_parallel
+    from oracle.cpu_baseline import make_pool, run_parallel, single_process_default_threads
     pool = make_pool(workers)
     try:
         run_parallel(8, 2, 4, CUTOFF, workers, seed=SEED, pool=pool)  # spawn + import outside the timing
@@ -403,10 +412,14 @@ def cpu_baseline_sample(workers: int):
     finally:
         pool.close()
         pool.join()
+    one = single_process_default_threads(CHI, 40, SEED)
     return {"value": round(r["updates_per_s"], 3), "unit": UNIT, "cores": workers, "kind": "port",
             "sample": (f"{workers} single-BLAS-thread processes, each one full n={N_SITES} depth-{DEPTH} "
                        f"chi={CHI} circuit ({r['updates']} updates, {r['wall_s']:.1f} s wall); oracle "
-                       "restatement of mps_core.py with scipy gesdd")}
+                       "restatement of mps_core.py with scipy gesdd"),
+            "single_process_default_threads": {
+                "value": round(one["updates_per_s"], 3), "unit": UNIT,
+                "sample": f"{one['updates']} saturated chi={CHI} updates in one process, default BLAS threads"}}
 
 
 def run_reference(args) -> None:

@@ -128,3 +128,67 @@ def run_grad_parallel(n: int, layers: int, chi: int, cutoff: float, workers: int
     vecs = sum(r[0] for r in res)
     return {"vectors": vecs, "wall_s": wall, "vectors_per_s": vecs / wall,
             "per_worker_s": float(np.mean([r[1] for r in res])), "workers": workers}
+
+
+def _fwd_worker(args) -> Tuple[int, float]:
+    n, layers, chi, cutoff, seed = args
+    try:
+        from threadpoolctl import threadpool_limits
+        limiter = threadpool_limits(1)
+    except Exception:  # pragma: no cover
+        limiter = None
+    import sys
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if here not in sys.path:
+        sys.path.insert(0, here)
+    from oracle.mps_adjoint import hea_energy, tfim_mpo
+    rng = np.random.default_rng(seed)
+    angles = rng.uniform(0.0, 2.0 * math.pi, size=(layers, n, 2))
+    t0 = time.perf_counter()
+    hea_energy(angles, tfim_mpo(n), chi, cutoff)
+    dt = time.perf_counter() - t0
+    del limiter
+    return 1, dt
+
+
+def run_forward_parallel(n: int, layers: int, chi: int, cutoff: float, workers: int, seed: int = 0,
+                         pool=None) -> Dict[str, float]:
+    """One ansatz energy evaluation (forward only, the unit of a parameter-shift
+    gradient) per worker process; returns the mean seconds per evaluation."""
+    own = pool is None
+    if own:
+        pool = mp.get_context("spawn").Pool(workers)
+    try:
+        res = pool.map(_fwd_worker, [(n, layers, chi, cutoff, seed + w) for w in range(workers)])
+    finally:
+        if own:
+            pool.close()
+            pool.join()
+    return {"s_per_eval": float(np.mean([r[1] for r in res])), "workers": workers}
+
+
+def _default_threads_worker(args) -> Tuple[int, float]:
+    chi, count, seed = args
+    import sys
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    if here not in sys.path:
+        sys.path.insert(0, here)
+    from oracle.mps_oracle import OracleMPS
+    rng = np.random.default_rng(seed)
+    st = OracleMPS(4, chi, 1e-10, record=False)
+    for k, (l, r) in enumerate([(1, chi), (chi, chi), (chi, chi), (chi, 1)]):
+        st.sites[k] = rng.standard_normal((l, 2, r)) + 1j * rng.standard_normal((l, 2, r))
+    gates = [_haar(rng) for _ in range(count)]
+    t0 = time.perf_counter()
+    for g in gates:
+        st.apply_adjacent_2q(1, g)  # a saturated chi x chi x chi update every time
+    return count, time.perf_counter() - t0
+
+
+def single_process_default_threads(chi: int = 64, count: int = 40, seed: int = 0) -> Dict[str, float]:
+    """Saturated two-site updates in one process with the BLAS library's default
+    thread count (the reference run as-is), in a spawned child."""
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        k, dt = pool.map(_default_threads_worker, [(chi, count, seed)])[0]
+    return {"updates": k, "seconds": dt, "updates_per_s": k / dt}
