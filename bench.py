@@ -620,7 +620,7 @@ def run_ours(args) -> None:
     if not args.quick and not args.no_gradient:
         from oracle.cpu_baseline import usable_cores
         cw = usable_cores() if (rank == 0 and world == 1 and not args.no_cpu) else 0
-        gradient = gradient_leg(dev, 3, 2, rank, max_over_ranks, cpu_workers=cw)
+        gradient = gradient_leg(dev, 5, 3, rank, max_over_ranks, cpu_workers=cw)
 
     reps.close()
     if rank != 0:
