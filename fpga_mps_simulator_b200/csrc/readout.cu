@@ -6,6 +6,7 @@
 // expectations: left/right transfer environments (the contraction of
 //               mps_core.py:364, trace-normalised per site) and local terms.
 #include "mpsb_common.cuh"
+#include "cta_gemm.cuh"
 
 namespace mpsb {
 
@@ -407,9 +408,11 @@ int launch_expect(const mpsb_chain *chains, int nchains, int n, int chi_cap, con
 // <a|b> of two chains of equal length: E_{k+1}[c, d] = sum_{x,y,s}
 // conj(A_k[x,s,c]) E_k[x,y] B_k[y,s,d], rescaled by its largest magnitude
 // each site (the scale is returned as a log).  One CTA; T in global scratch.
-__global__ void overlap_kernel(const mpsb_chain *pa, const mpsb_chain *pb, int n, int chi_cap, double2 *out,
-                               double *out_log, double2 *tscr) {
+__global__ void __launch_bounds__(kCtaGemmThreads, 1)
+    overlap_kernel(const mpsb_chain *pa, const mpsb_chain *pb, int n, int chi_cap, double2 *out, double *out_log,
+                   double2 *tscr) {
     extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ GemmSmem gsm;
     double2 *E = reinterpret_cast<double2 *>(sm);
     double2 *En = E + chi_cap * chi_cap;
     __shared__ double red[32];
@@ -422,25 +425,21 @@ __global__ void overlap_kernel(const mpsb_chain *pa, const mpsb_chain *pb, int n
         const int cla = a.bonds[k], cra = a.bonds[k + 1], clb = b.bonds[k], crb = b.bonds[k + 1];
         const double2 *A = reinterpret_cast<const double2 *>(a.sites + (size_t)k * a.slot_elems);
         const double2 *B = reinterpret_cast<const double2 *>(b.sites + (size_t)k * b.slot_elems);
-        for (int e = tid; e < cla * 2 * crb; e += nth) {  // T[x, t, d] = sum_y E[x, y] B[y, t, d]
-            const int x = e / (2 * crb), rem = e - x * 2 * crb;
-            double2 acc = make_double2(0, 0);
-            for (int y = 0; y < clb; ++y) acc = c_fma(E[x * clb + y], B[(size_t)y * 2 * crb + rem], acc);
-            tscr[e] = acc;
-        }
-        __threadfence_block();
-        __syncthreads();
+        // T[x, (t, d)] = sum_y E[x, y] B[y, (t, d)]
+        cta_cgemm<true, true>(
+            cla, 2 * crb, clb, [&](int i, int kk) { return E[i * clb + kk]; },
+            [&](int kk, int j) { return B[(size_t)kk * 2 * crb + j]; },
+            [&](int i, int j, double2 v) { tscr[(size_t)i * 2 * crb + j] = v; }, gsm);
+        // E'[c, d] = sum_{(x, s)} conj(A[(x, s), c]) T[(x, s), d]
         double part = 0.0;
-        for (int e = tid; e < cra * crb; e += nth) {  // E'[c, d] = sum_{x,s} conj(A[x,s,c]) T[x,s,d]
-            const int c = e / crb, d = e - c * crb;
-            double2 acc = make_double2(0, 0);
-            for (int x = 0; x < cla; ++x) {
-                acc = c_cfma(A[(size_t)(2 * x) * cra + c], tscr[(size_t)(2 * x) * crb + d], acc);
-                acc = c_cfma(A[(size_t)(2 * x + 1) * cra + c], tscr[(size_t)(2 * x + 1) * crb + d], acc);
-            }
-            En[e] = acc;
-            part = fmax(part, c_abs2(acc));
-        }
+        cta_cgemm<false, true>(
+            cra, crb, 2 * cla, [&](int i, int kk) { return c_conj(A[(size_t)kk * cra + i]); },
+            [&](int kk, int j) { return tscr[(size_t)kk * crb + j]; },
+            [&](int i, int j, double2 v) {
+                En[i * crb + j] = v;
+                part = fmax(part, c_abs2(v));
+            },
+            gsm);
         // block max
         for (int o = 16; o > 0; o >>= 1) part = fmax(part, __shfl_xor_sync(0xffffffffu, part, o));
         if ((tid & 31) == 0) red[tid >> 5] = part;
@@ -468,7 +467,7 @@ int launch_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap,
             return check_launch("cudaFuncSetAttribute(overlap)");
         configured = smem;
     }
-    overlap_kernel<<<1, 256, smem, s>>>(a, b, n, chi_cap, out, out_log, reinterpret_cast<double2 *>(ws));
+    overlap_kernel<<<1, kCtaGemmThreads, smem, s>>>(a, b, n, chi_cap, out, out_log, reinterpret_cast<double2 *>(ws));
     return check_launch("overlap_kernel");
 }
 
