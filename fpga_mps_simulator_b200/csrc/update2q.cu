@@ -259,11 +259,41 @@ __device__ __forceinline__ int rotate4(double2 (&x0)[RPL], double2 (&y0)[RPL], d
     const double a = j == 0 ? a0 : (j == 1 ? a1 : (j == 2 ? a2 : a3));
     const double b = j == 0 ? b0 : (j == 1 ? b1 : (j == 2 ? b2 : b3));
     const Rot mine = jacobi_rotation(a, b, kr, ki, tol2);
-    int n = apply_one<RPL>(x0, y0, a0, b0, mine, 0);
-    n += apply_one<RPL>(x1, y1, a1, b1, mine, 8);
-    n += apply_one<RPL>(x2, y2, a2, b2, mine, 16);
-    n += apply_one<RPL>(x3, y3, a3, b3, mine, 24);
-    return n;
+    if constexpr (RPL >= 4) {
+        // 128 rows: register-bound, so one rotation's norms at a time
+        int n = apply_one<RPL>(x0, y0, a0, b0, mine, 0);
+        n += apply_one<RPL>(x1, y1, a1, b1, mine, 8);
+        n += apply_one<RPL>(x2, y2, a2, b2, mine, 16);
+        n += apply_one<RPL>(x3, y3, a3, b3, mine, 24);
+        return n;
+    } else {
+        // <= 64 rows: all four applies in one straight run, then one warp vote
+        // for the rare norm recompute (11-12 % faster at chi = 32)
+        const Rot q0 = shfl_rot_from(mine, 0), q1 = shfl_rot_from(mine, 8);
+        const Rot q2 = shfl_rot_from(mine, 16), q3 = shfl_rot_from(mine, 24);
+        apply_rot<RPL>(x0, y0, q0);
+        apply_rot<RPL>(x1, y1, q1);
+        apply_rot<RPL>(x2, y2, q2);
+        apply_rot<RPL>(x3, y3, q3);
+        const double a0n = a0 - q0.dl, b0n = b0 + q0.dl, a1n = a1 - q1.dl, b1n = b1 + q1.dl;
+        const double a2n = a2 - q2.dl, b2n = b2 + q2.dl, a3n = a3 - q3.dl, b3n = b3 + q3.dl;
+        const bool c0 = a0n < 1e-8 * a0, d0 = b0n < 1e-8 * b0, c1 = a1n < 1e-8 * a1, d1 = b1n < 1e-8 * b1;
+        const bool c2 = a2n < 1e-8 * a2, d2 = b2n < 1e-8 * b2, c3 = a3n < 1e-8 * a3, d3 = b3n < 1e-8 * b3;
+        if (__any_sync(0xffffffffu, c0 | d0 | c1 | d1 | c2 | d2 | c3 | d3)) {
+            a0 = c0 ? col_norm2<RPL>(x0) : a0n;
+            b0 = d0 ? col_norm2<RPL>(y0) : b0n;
+            a1 = c1 ? col_norm2<RPL>(x1) : a1n;
+            b1 = d1 ? col_norm2<RPL>(y1) : b1n;
+            a2 = c2 ? col_norm2<RPL>(x2) : a2n;
+            b2 = d2 ? col_norm2<RPL>(y2) : b2n;
+            a3 = c3 ? col_norm2<RPL>(x3) : a3n;
+            b3 = d3 ? col_norm2<RPL>(y3) : b3n;
+        } else {
+            a0 = a0n; b0 = b0n; a1 = a1n; b1 = b1n;
+            a2 = a2n; b2 = b2n; a3 = a3n; b3 = b3n;
+        }
+        return (q0.dl != 0.0) + (q1.dl != 0.0) + (q2.dl != 0.0) + (q3.dl != 0.0);
+    }
 }
 
 // Column quads in registers: quad q of slot s is columns 4q..4q+3.
