@@ -43,7 +43,7 @@ WORKLOAD = (f"MPS two-site updates: n={N_SITES} open chain, depth-{DEPTH} Haar b
 
 # DRAM bytes (read + write) of one saturated-layer launch of the update kernel
 # (49 pairs at chi = 64, mixed form), from one ncu capture of this workload.
-TRAFFIC_PER_LAUNCH = 12.04e6
+TRAFFIC_PER_LAUNCH = 11.99e6
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum, layer 19 of config 2 "
                   "(profiles/update2q_n100_chi64_mixed_and_fp64.md); algorithmic site reads 12.8 MB")
 
