@@ -195,6 +195,28 @@ __device__ __forceinline__ Rot shfl_rot_from(const Rot &r, int src) {
     return o;
 }
 
+// The four rotations of a phase, from lanes 0, 8, 16, 24 to every lane,
+// through a small per-warp shared-memory buffer (two 16-byte stores by the
+// owners, eight broadcast 16-byte loads) instead of 32 shuffles: 3-6 %
+// faster at <= 64 rows; at 128 rows the extra registers spill, so that path
+// keeps the shuffles.
+constexpr int kRotBufWarps = kUpdThreads / 32;
+__device__ __forceinline__ void bcast_rots(const Rot &mine, int lane, Rot &q0, Rot &q1, Rot &q2, Rot &q3) {
+    __shared__ double2 rotbuf[kRotBufWarps][4][2];
+    double2(*buf)[2] = rotbuf[threadIdx.x >> 5];
+    if ((lane & 7) == 0) {
+        buf[lane >> 3][0] = make_double2(mine.c, mine.sr);
+        buf[lane >> 3][1] = make_double2(mine.si, mine.dl);
+    }
+    __syncwarp();
+    double2 u, v;
+    u = buf[0][0]; v = buf[0][1]; q0.c = u.x; q0.sr = u.y; q0.si = v.x; q0.dl = v.y;
+    u = buf[1][0]; v = buf[1][1]; q1.c = u.x; q1.sr = u.y; q1.si = v.x; q1.dl = v.y;
+    u = buf[2][0]; v = buf[2][1]; q2.c = u.x; q2.sr = u.y; q2.si = v.x; q2.dl = v.y;
+    u = buf[3][0]; v = buf[3][1]; q3.c = u.x; q3.sr = u.y; q3.si = v.x; q3.dl = v.y;
+    __syncwarp();  // every lane has read before the next phase writes
+}
+
 // Two broadcast rotations applied back to back; the norms follow
 // a' = a - t|g|, b' = b + t|g| and are recomputed from the data only when one
 // of them cancels (below 1e-8 of its old value), decided by one warp vote so
@@ -203,8 +225,7 @@ __device__ __forceinline__ Rot shfl_rot_from(const Rot &r, int src) {
 template <int RPL>
 __device__ __forceinline__ int apply_two(double2 (&x0)[RPL], double2 (&y0)[RPL], double &a0, double &b0,
                                          double2 (&x1)[RPL], double2 (&y1)[RPL], double &a1, double &b1,
-                                         const Rot &mine, int s0, int s1) {
-    const Rot q0 = shfl_rot_from(mine, s0), q1 = shfl_rot_from(mine, s1);
+                                         const Rot &q0, const Rot &q1) {
     apply_rot<RPL>(x0, y0, q0);
     apply_rot<RPL>(x1, y1, q1);
     const double a0n = a0 - q0.dl, b0n = b0 + q0.dl, a1n = a1 - q1.dl, b1n = b1 + q1.dl;
@@ -261,14 +282,14 @@ __device__ __forceinline__ int rotate4(double2 (&x0)[RPL], double2 (&y0)[RPL], d
     if constexpr (RPL >= 4) {
         // 128 rows: register-bound, so two rotations per vote (8 % faster than
         // one, while four at a time spills into a 40 % slowdown)
-        int n = apply_two<RPL>(x0, y0, a0, b0, x1, y1, a1, b1, mine, 0, 8);
-        n += apply_two<RPL>(x2, y2, a2, b2, x3, y3, a3, b3, mine, 16, 24);
+        int n = apply_two<RPL>(x0, y0, a0, b0, x1, y1, a1, b1, shfl_rot_from(mine, 0), shfl_rot_from(mine, 8));
+        n += apply_two<RPL>(x2, y2, a2, b2, x3, y3, a3, b3, shfl_rot_from(mine, 16), shfl_rot_from(mine, 24));
         return n;
     } else {
         // <= 64 rows: all four applies in one straight run, then one warp vote
         // for the rare norm recompute (11-12 % faster at chi = 32)
-        const Rot q0 = shfl_rot_from(mine, 0), q1 = shfl_rot_from(mine, 8);
-        const Rot q2 = shfl_rot_from(mine, 16), q3 = shfl_rot_from(mine, 24);
+        Rot q0, q1, q2, q3;
+        bcast_rots(mine, lane, q0, q1, q2, q3);
         apply_rot<RPL>(x0, y0, q0);
         apply_rot<RPL>(x1, y1, q1);
         apply_rot<RPL>(x2, y2, q2);
