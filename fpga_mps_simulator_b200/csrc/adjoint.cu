@@ -8,8 +8,8 @@
 // complex array z is z_bar = dL/dRe z + i dL/dIm z, so y = W x gives
 // x_bar = W^H y_bar.
 //
-// Two-site update backward (one CTA per pair).  The forward's Jacobi
-// factorised X = theta (or theta^H when chi_r > chi_l), R x C with R >= C,
+// Two-site update backward (persistent grid, one pair per CTA at a time).
+// The forward's Jacobi factorised X = theta (or theta^H when chi_r > chi_l), R x C with R >= C,
 // as X = U S V^H; the tape holds X, the converged columns u_k S_k in
 // decreasing order of S_k, and the spectrum.  The kept triplets carry the
 // cotangents, the discarded ones none; the exact derivative is the thin-SVD
@@ -26,10 +26,13 @@
 // The cotangents of the sqrt(S) split and of the kept-norm renormalisation
 // give U_bar, V_bar and S_bar; then theta_bar = G^H M_bar, A_bar = theta_bar
 // B^H and B_bar = A^H theta_bar.  All matrices of one pair live in a
-// per-pair global scratch (L2-resident at these sizes) and are combined by a
+// per-CTA global scratch (L2-resident at these sizes) and are combined by a
 // 64 x 64 tiled complex FP64 GEMM run by the whole CTA.
 #include "mpsb_common.cuh"
 #include "cta_gemm.cuh"
+
+#include <algorithm>
+#include <climits>
 
 namespace mpsb {
 
@@ -53,13 +56,14 @@ struct BwdParams {
     double broaden;
 };
 
-__global__ void __launch_bounds__(kBwdThreads, 1) update2q_backward_kernel(const BwdParams p) {
+// One pair; every early exit is block-uniform.  `base` is this CTA's scratch.
+__device__ __forceinline__ void backward_pair(const BwdParams &p, const int pi, double2 *base) {
     __shared__ GemmSmem sm;
     __shared__ double sS[128], sSb[128];
     __shared__ int s_rp, s_bad;
     __shared__ double2 s_gate[16];
     __shared__ double2 s_red[kBwdThreads / 32][16];
-    const int pi = blockIdx.x, tid = threadIdx.x;
+    const int tid = threadIdx.x;
     const mpsb_pair pr = p.pairs[pi];
     const mpsb_chain ch = p.pre[pr.chain];
     const mpsb_chain cc = p.cot[pr.chain];
@@ -114,7 +118,6 @@ __global__ void __launch_bounds__(kBwdThreads, 1) update2q_backward_kernel(const
     const double2 *Asite = reinterpret_cast<const double2 *>(ch.sites + (size_t)site * ch.slot_elems);
     const double2 *Bsite = reinterpret_cast<const double2 *>(ch.sites + (size_t)(site + 1) * ch.slot_elems);
 
-    double2 *base = p.ws + (size_t)pi * p.ws_stride;
     double2 *U = base;                       // R x rp
     double2 *V = base + Qn;                  // C x rp
     double2 *Ub = base + 2 * Qn;             // R x K
@@ -288,6 +291,17 @@ __global__ void __launch_bounds__(kBwdThreads, 1) update2q_backward_kernel(const
             [&](int i, int j, double2 v) { Bcot[(size_t)i * twocr + j] = v; }, sm);
     }
     if (tid == 0) p.status[pr.out] = 0;
+}
+
+// Persistent grid (one CTA per SM at most): a CTA walks pairs blockIdx.x,
+// blockIdx.x + gridDim.x, ... and reuses ONE scratch region, so the live
+// scratch is gridDim.x regions (L2-resident) instead of one per pair.
+__global__ void __launch_bounds__(kBwdThreads, 1) update2q_backward_kernel(const BwdParams p) {
+    double2 *base = p.ws + (size_t)blockIdx.x * p.ws_stride;
+    for (int pi = blockIdx.x; pi < p.npairs; pi += gridDim.x) {
+        backward_pair(p, pi, base);
+        __syncthreads();  // shared tiles and scratch are reused by the next pair
+    }
 }
 
 // ------------------------------------------------------------------ one-site
@@ -569,9 +583,28 @@ __global__ void __launch_bounds__(kBwdThreads, 1) mpo_grad_kernel(const GradPara
 // ------------------------------------------------------------------ host
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// CTAs of the persistent backward grid: every resident CTA on the device
+// (no cap while no device answers the query).
+static int bwd_grid_cap() {
+    static int cap = 0;
+    if (cap == 0) {
+        int dev = 0, sms = 0, per_sm = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, update2q_backward_kernel, kBwdThreads, 0) !=
+                cudaSuccess ||
+            sms < 1 || per_sm < 1) {
+            cudaGetLastError();
+            return INT_MAX;
+        }
+        cap = sms * per_sm;
+    }
+    return cap;
+}
+
 size_t bwd_workspace_bytes(int npairs, int chi_cap) {
     const size_t q = (size_t)(2 * chi_cap) * (2 * chi_cap);
-    return (size_t)npairs * 8 * q * sizeof(double2);
+    return (size_t)std::min(npairs, bwd_grid_cap()) * 8 * q * sizeof(double2);
 }
 
 int launch_update2q_backward(const mpsb_chain *pre, const mpsb_chain *cot, const mpsb_pair *pairs, int npairs,
@@ -593,7 +626,7 @@ int launch_update2q_backward(const mpsb_chain *pre, const mpsb_chain *cot, const
     p.chi_cap = chi_cap;
     p.retain = retain;
     p.broaden = broaden;
-    update2q_backward_kernel<<<npairs, kBwdThreads, 0, s>>>(p);
+    update2q_backward_kernel<<<std::min(npairs, bwd_grid_cap()), kBwdThreads, 0, s>>>(p);
     return check_launch("update2q_backward_kernel");
 }
 

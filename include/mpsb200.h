@@ -254,7 +254,9 @@ MPSB_API int mpsb_update2q_batch_taped(const mpsb_chain *chains, const mpsb_pair
                                        double *spectra, int32_t *kept, double *trunc, int32_t *status,
                                        mpsb_stream_t stream);
 
-/* Bytes of device workspace mpsb_update2q_backward_batch needs. */
+/* Bytes of device workspace mpsb_update2q_backward_batch needs: one scratch
+ * region of 8 (2 chi_cap)^2 complex per CTA, min(npairs, CTAs resident on the
+ * current device).  Call with the device of the launch current. */
 MPSB_API size_t mpsb_update2q_backward_workspace_bytes(int npairs, int chi_cap);
 
 /* Backward of one taped call: for every pair, the cotangents of the updated
