@@ -143,17 +143,31 @@ __device__ __forceinline__ void backward_pair(const BwdParams &p, const int pi, 
             dB[e] = c_scale(c_conj(Bcot[(size_t)k * twocr + col]), sqrt(sS[k] / div));
         }
     }
-    // 2. U = Xs / S
-    for (int e = tid; e < R * rp; e += kBwdThreads) {
-        const int r = e / rp, j = e - r * rp;
-        U[e] = c_scale(Xs[(size_t)j * R + r], 1.0 / sS[j]);
+    if (meta[kTapeMetaSide] != 0.0) {
+        // 2'. V = Vs / S (the QR-preconditioned forward taped the right side)
+        for (int e = tid; e < C * rp; e += kBwdThreads) {
+            const int i = e / rp, j = e - i * rp;
+            V[e] = c_scale(Xs[(size_t)j * C + i], 1.0 / sS[j]);
+        }
+        __syncthreads();
+        // 3'. U = X V S^-1   (R x rp)
+        cta_cgemm<true, true>(
+            R, rp, C, [&](int r, int k) { return X[(size_t)r * C + k]; },
+            [&](int k, int j) { return V[(size_t)k * rp + j]; },
+            [&](int r, int j, double2 v) { U[(size_t)r * rp + j] = c_scale(v, 1.0 / sS[j]); }, sm);
+    } else {
+        // 2. U = Xs / S
+        for (int e = tid; e < R * rp; e += kBwdThreads) {
+            const int r = e / rp, j = e - r * rp;
+            U[e] = c_scale(Xs[(size_t)j * R + r], 1.0 / sS[j]);
+        }
+        __syncthreads();
+        // 3. V = X^H U S^-1   (C x rp)
+        cta_cgemm<false, true>(
+            C, rp, R, [&](int i, int k) { return c_conj(X[(size_t)k * C + i]); },
+            [&](int k, int j) { return U[(size_t)k * rp + j]; },
+            [&](int i, int j, double2 v) { V[(size_t)i * rp + j] = c_scale(v, 1.0 / sS[j]); }, sm);
     }
-    __syncthreads();
-    // 3. V = X^H U S^-1   (C x rp)
-    cta_cgemm<false, true>(
-        C, rp, R, [&](int i, int k) { return c_conj(X[(size_t)k * C + i]); },
-        [&](int k, int j) { return U[(size_t)k * rp + j]; },
-        [&](int i, int j, double2 v) { V[(size_t)i * rp + j] = c_scale(v, 1.0 / sS[j]); }, sm);
     // 4. P = U^H U_bar, Q = V^H V_bar   (rp x K)
     cta_cgemm<false, true>(
         rp, K, R, [&](int i, int k) { return c_conj(U[(size_t)k * rp + i]); },

@@ -66,14 +66,17 @@ struct PairRec {
 
 // Adjoint tape of one two-site update, per pair, in double2 units with
 // Q = (2 chi_cap)^2:
-//   [0, Q)       X, the matrix the Jacobi orthogonalised (theta, or theta^H
-//                when chi_r > chi_l), R x C row-major
-//   [Q, 2Q)      the converged columns of X (u_k S_k) in decreasing order of
-//                S_k, column k at [Q + k R, Q + (k + 1) R)
+//   [0, Q)       X = U S V^H, the matrix the update factorised (theta, or
+//                theta^H when chi_r > chi_l), R x C row-major
+//   [Q, 2Q)      singular vectors times S in decreasing order of S_k: either
+//                u_k S_k at [Q + k R, Q + (k + 1) R), or (side flag set, the
+//                QR-preconditioned factorisation) v_k S_k at
+//                [Q + k C, Q + (k + 1) C)
 //   [2Q, 2Q+72)  144 doubles: S[0..128), then keep, the kept-norm divisor,
-//                R and C
+//                R, C and the side flag
 // rounded up to a multiple of 16 double2 (256 bytes).
 constexpr int kTapeMetaKeep = 128, kTapeMetaDiv = 129, kTapeMetaRows = 130, kTapeMetaCols = 131;
+constexpr int kTapeMetaSide = 132;
 __host__ __device__ inline long long tape_stride(int chi_cap) {
     const long long q = (long long)(2 * chi_cap) * (2 * chi_cap);
     return (2 * q + 72 + 15) & ~15LL;
