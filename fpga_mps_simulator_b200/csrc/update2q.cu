@@ -572,8 +572,12 @@ __device__ __forceinline__ double2 householder(double2 (&x)[RPL], int k, int lan
     double2 tau = make_double2(0.0, 0.0);
     double beta = al.x;
     if (xn2 > 0.0 || al.y != 0.0) {
-        beta = -copysign(sqrt(fma(al.x, al.x, fma(al.y, al.y, xn2))), al.x);
-        tau = make_double2((beta - al.x) / beta, -al.y / beta);
+        const double n2 = fma(al.x, al.x, fma(al.y, al.y, xn2));
+        const double rn = rsqrt(n2);
+        const double sg = signbit(al.x) ? 1.0 : -1.0;  // beta takes the sign opposite to Re(alpha)
+        beta = sg * n2 * rn;
+        const double ib = sg * rn;  // 1 / beta
+        tau = make_double2((beta - al.x) * ib, -al.y * ib);
         const double dx = al.x - beta, dy = al.y;
         const double id2 = 1.0 / fma(dx, dx, dy * dy);
         const double2 sc = make_double2(dx * id2, -dy * id2);  // 1 / (alpha - beta)
@@ -683,18 +687,21 @@ __device__ __forceinline__ void factor_panel(double2 (&X)[4][RPL], int k0, int l
 // lane l ends with product l) and shared through the warp's scratch row.
 template <int RPL>
 __device__ __forceinline__ void apply_panel(double2 (&Y)[4][RPL], const double2 *vb, const double2 *tb, double *wred, int lane,
-                            int rpad) {
+                            int rpad, int k0) {
+    // register rows wholly above the panel meet only zeros of V (warp-uniform)
+    const int u0 = k0 >> 5;
     double v[32];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
         double2 vi[RPL];
 #pragma unroll
-        for (int u = 0; u < RPL; ++u) vi[u] = vb[i * rpad + lane + 32 * u];
+        for (int u = 0; u < RPL; ++u) vi[u] = u >= u0 ? vb[i * rpad + lane + 32 * u] : make_double2(0.0, 0.0);
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-            for (int u = 0; u < RPL; ++u) acc = c_cfma(vi[u], Y[c][u], acc);
+            for (int u = 0; u < RPL; ++u)
+                if (u >= u0) acc = c_cfma(vi[u], Y[c][u], acc);
             v[2 * (4 * i + c)] = acc.x;
             v[2 * (4 * i + c) + 1] = acc.y;
         }
@@ -733,6 +740,7 @@ __device__ __forceinline__ void apply_panel(double2 (&Y)[4][RPL], const double2 
     for (int i = 0; i < 4; ++i) {
 #pragma unroll
         for (int u = 0; u < RPL; ++u) {
+            if (u < u0) continue;
             const double2 vi = vb[i * rpad + lane + 32 * u];
 #pragma unroll
             for (int c = 0; c < 4; ++c) Y[c][u] = c_sub(Y[c][u], c_mul(vi, Zc[i][c]));
@@ -842,21 +850,30 @@ __device__ void qr_factor(cg::cluster_group &cluster, const Slots &S, double2 *v
     double nr[4];
     if (has0) load_quad<RPL>(S, (4 * lq0) / w, ((4 * lq0) % w) >> 2, lane, Q0, nr);
     if (has1) load_quad<RPL>(S, (4 * lq1) / w, ((4 * lq1) % w) >> 2, lane, Q1, nr);
-    for (int p = 0; p < npanels; ++p) {
+    // CTA 0's panels are needed by both CTAs (cluster barriers); CTA 1's own
+    // panels only by CTA 1 (block barriers; CTA 0 has nothing left to do).
+    const int nshared = min(npanels, nqc);
+    const int pend = crank == 0 ? nshared : npanels;
+    for (int p = 0; p < pend; ++p) {
+        const bool shared = p < nshared;
         const int oc = p / nqc, olq = p - oc * nqc;
         double2 *vb = vbuf + (p & 1) * 4 * rpad;
-        double2 *vbp = vbuf_peer + (p & 1) * 4 * rpad;
         double2 *tb = &qs->tbuf[p & 1][0];
-        double2 *tbp = tb_peer + (p & 1) * 16;
+        // CTA 1's own panels are published to itself only (both copies local)
+        double2 *vbp = shared ? vbuf_peer + (p & 1) * 4 * rpad : vb;
+        double2 *tbp = shared ? tb_peer + (p & 1) * 16 : tb;
         if (oc == crank && olq % kWarps == warp) {
             if (olq == lq0)
                 factor_panel<RPL>(Q0, 4 * p, lane, rpad, vb, vbp, tb, tbp);
             else
                 factor_panel<RPL>(Q1, 4 * p, lane, rpad, vb, vbp, tb, tbp);
         }
-        cluster.sync();  // panel p published in both CTAs
-        if (has0 && gp0 > p) apply_panel<RPL>(Q0, vb, tb, wred, lane, rpad);
-        if (has1 && gp1 > p) apply_panel<RPL>(Q1, vb, tb, wred, lane, rpad);
+        if (shared)
+            cluster.sync();  // panel p published in both CTAs
+        else
+            __syncthreads();  // panel p published in CTA 1
+        if (has0 && gp0 > p) apply_panel<RPL>(Q0, vb, tb, wred, lane, rpad, 4 * p);
+        if (has1 && gp1 > p) apply_panel<RPL>(Q1, vb, tb, wred, lane, rpad, 4 * p);
     }
     const double nz[4] = {0.0, 0.0, 0.0, 0.0};
     if (has0) store_quad<RPL>(S, (4 * lq0) / w, ((4 * lq0) % w) >> 2, lane, Q0, nz);
