@@ -749,12 +749,14 @@ __device__ __forceinline__ void apply_panel(double2 (&Y)[4][RPL], const double2 
 }
 
 // The preconditioner pays where the column norms of theta spread (graded
-// spectra: the CZ ansatz, Trotter evolution; min/max |x_j|^2 below 5e-3 for
+// spectra: the CZ ansatz, Trotter evolution; min/max |x_j|^2 near 4e-4 for
 // most of their updates) and costs more than the sweeps it saves on random
-// brickwork (ratios 0.01-0.3): measured 17.6 -> 11.5 sweeps at chi = 32 on
-// the ansatz, 11.5 -> 9.9 at chi = 64 on brickwork for a QR costing ~2.3
-// sweeps there.
-constexpr double kPrecondSpread = 5e-3;
+// brickwork (ratios 0.01-0.3, median 0.15): measured 17.6 -> 11.5 sweeps at
+// chi = 32 on the ansatz, 11.5 -> 9.9 at chi = 64 on brickwork for a QR
+// costing ~2.3 sweeps there.  A 2e-2 gate was 2 % faster than 5e-3 on the
+// ansatz (fewer slow unpreconditioned pairs in each wave) and within noise
+// on brickwork.
+constexpr double kPrecondSpread = 2e-2;
 
 // Decide whether to precondition (both CTAs reach the same answer from the
 // same keys).  If so, sort the columns by decreasing norm (ties by column
