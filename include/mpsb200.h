@@ -239,8 +239,10 @@ MPSB_API int mpsb_canonicalize(const mpsb_chain *chains, const int32_t *chain_id
  * the state's (only its sites and slot_elems fields are read); the shapes
  * come from the bonds of the `pre` table, the state before the op. */
 
-/* Bytes of tape mpsb_update2q_batch_taped writes for npairs pairs (theta as
- * the Jacobi saw it, the converged Jacobi columns and the spectrum). */
+/* Bytes of tape mpsb_update2q_batch_taped writes for npairs pairs (theta or
+ * theta^H as factorised, one side's singular vectors times S -- the left
+ * side, or the right side with a flag for pairs the QR preconditioner
+ * handled -- and the spectrum). */
 MPSB_API size_t mpsb_update2q_tape_bytes(int npairs, int chi_cap);
 
 /* mpsb_update2q_batch that also records the tape of every pair (pair q at

@@ -10,7 +10,7 @@ import pytest
 import torch
 
 from oracle.mps_adjoint import (apply1q_backward, hea_energy_grad, mpo_energy_grad, tfim_mpo as oracle_tfim,
-                                update_backward_given_outputs)
+                                update_backward_given_outputs, update_forward)
 
 pytestmark = pytest.mark.gpu
 REL = 1e-9
@@ -39,23 +39,32 @@ def _get(t, b, k, shape):
     return t[_slot(b, k), : int(np.prod(shape))].cpu().numpy().reshape(shape)
 
 
-@pytest.mark.parametrize("cl,cm,cr,chi,cut,gate_kind", [
-    (4, 8, 4, 64, 1e-12, "haar"),      # square, no truncation
-    (8, 8, 2, 64, 1e-12, "haar"),      # tall theta (Jacobi on theta)
-    (2, 8, 8, 64, 1e-12, "haar"),      # wide theta (Jacobi on theta^H)
-    (4, 4, 4, 4, 1e-12, "haar"),       # chi truncation with kept/discarded coupling
-    (16, 16, 16, 16, 1e-12, "general"),  # non-unitary gate, truncation
-    (32, 32, 32, 32, 1e-12, "haar"),   # chi = 32 saturated layer shape
-    (64, 64, 64, 64, 1e-10, "haar"),   # chi = 64, 128 x 128 theta
+@pytest.mark.parametrize("cl,cm,cr,chi,cut,gate_kind,graded", [
+    (4, 8, 4, 64, 1e-12, "haar", False),      # square, no truncation
+    (8, 8, 2, 64, 1e-12, "haar", False),      # tall theta (Jacobi on theta)
+    (2, 8, 8, 64, 1e-12, "haar", False),      # wide theta (Jacobi on theta^H)
+    (4, 4, 4, 4, 1e-12, "haar", False),       # chi truncation with kept/discarded coupling
+    (16, 16, 16, 16, 1e-12, "general", False),  # non-unitary gate, truncation
+    (32, 32, 32, 32, 1e-12, "haar", False),   # chi = 32 saturated layer shape
+    (64, 64, 64, 64, 1e-10, "haar", False),   # chi = 64, 128 x 128 theta
+    # graded theta: the QR-preconditioned path (Jacobi on R^H, right-side tape)
+    (16, 16, 16, 16, 1e-12, "haar", True),
+    (32, 32, 32, 32, 1e-12, "general", True),
+    (64, 64, 64, 64, 1e-10, "haar", True),
+    (12, 16, 24, 32, 1e-12, "haar", True),    # wide: preconditioned Jacobi on theta^H
+    (4, 8, 4, 64, 1e-12, "haar", True),       # too few columns for the preconditioner
 ])
-def test_update_backward_matches_oracle(cl, cm, cr, chi, cut, gate_kind):
+def test_update_backward_matches_oracle(cl, cm, cr, chi, cut, gate_kind, graded):
     from fpga_mps_simulator_b200 import MPSBatch, _lib
     from fpga_mps_simulator_b200.adjoint import AdjointEngine, Step2Q
     from fpga_mps_simulator_b200.hamiltonians import zz_mpo
-    rng = np.random.default_rng(cl * 1000 + cm * 10 + cr)
+    rng = np.random.default_rng(cl * 1000 + cm * 10 + cr + 7 * graded)
     n, i = 16, 7
     b = MPSBatch([n], [chi], [cut])
     A, B = _rand(rng, (cl, 2, cm)), _rand(rng, (cm, 2, cr))
+    if graded:  # column norms of theta (and of theta^H) spread over ~3 decades
+        A *= np.logspace(0.0, -1.5, cl)[:, None, None]
+        B *= np.logspace(0.0, -1.5, cr)[None, None, :]
     G = _haar(rng) if gate_kind == "haar" else _haar(rng) + 0.3 * _rand(rng, (4, 4))
     b.set_site(0, i, A)
     b.set_site(0, i + 1, B)
@@ -65,8 +74,18 @@ def test_update_backward_matches_oracle(cl, cm, cr, chi, cut, gate_kind):
     rec = eng._record(step)
     torch.cuda.synchronize()
     assert int(pb.status.item()) == 0
+    # tape side flag (meta double 132): set exactly when the pair was preconditioned
+    q = (2 * b.chi_cap) ** 2
+    side = float(rec[2].view(torch.float64)[4 * q + 132].item())
+    assert side == (1.0 if graded and 2 * min(cl, cr) > 16 else 0.0), side
     k = int(pb.kept.item())
     Ap, Bp = b.site(0, i), b.site(0, i + 1)
+    # forward parity on the gauge-invariant product A' B' and the kept count
+    rAp, rBp, aux = update_forward(A, B, G, chi, cut)
+    assert k == aux["keep"]
+    got_t = np.einsum("lpm,mqr->lpqr", Ap, Bp)
+    want_t = np.einsum("lpm,mqr->lpqr", rAp, rBp)
+    assert np.max(np.abs(got_t - want_t)) <= 1e-10 * max(1.0, np.max(np.abs(want_t)))
     Cb_a, Cb_b = _rand(rng, (cl, 2, k)), _rand(rng, (k, 2, cr))
     eng.cot.zero_()
     _put_cot(b, eng.cot, i, Cb_a)
