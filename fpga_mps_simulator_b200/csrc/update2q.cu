@@ -1424,10 +1424,12 @@ static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb
     p.wmax = (((2 * chi_cap) + 15) & ~15) / 4;
     p.tol2 = tol * tol;
     p.max_sweeps = max_sweeps;
-    // At chi_cap <= 16 a 128-row tensor-core tile is mostly padding and the
-    // FP64 contraction is both exact and faster (measured: 37 vs 55 ms per
-    // 64-vector ansatz forward), so the mixed form uses it there.
-    if (mixed && rpl == 1) mixed = false;
+    // At chi_cap <= 32 a 128-row tensor-core tile is half padding or more and
+    // the FP64 contraction is both exact and faster (measured per 64-vector
+    // ansatz forward: 37 vs 55 ms at chi = 16, 96.9 vs 104.9 ms at chi = 32),
+    // so the mixed form uses it there (and keeps only its looser Jacobi
+    // tolerance).
+    if (mixed && rpl <= 2) mixed = false;
     // 3xTF32 theta carries relative errors near 1e-7, so singular values below
     // ~1e-6 S[0] are rounding noise: the mixed form never keeps them
     p.cut_floor = mixed ? kMixedCutoffFloor : 0.0;

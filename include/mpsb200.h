@@ -79,9 +79,11 @@ enum mpsb_precision {
     MPSB_FP64 = 0,        /* complex128 end to end (the drop-in form)                    */
     MPSB_MIXED_TF32X3 = 1 /* theta by 3xTF32 complex-3M tensor-core GEMMs (tcgen05), FP64
                              Jacobi SVD; singular values below 1e-6 S[0] (theta's rounding
-                             floor) are never kept, whatever the cutoff.  At chi_cap <= 16
-                             the contraction runs in FP64 (exact, no floor): the tensor-core
-                             tile would be mostly padding                               */
+                             floor) are never kept, whatever the cutoff.  At chi_cap <= 32
+                             the contraction runs in FP64 (exact, no floor): the 128-row
+                             tensor-core tile would be half padding or more, and the form
+                             then differs from MPSB_FP64 only by its Jacobi tolerance
+                             (1e-9 against 1e-14)                                        */
 };
 
 enum mpsb_status_bits {
