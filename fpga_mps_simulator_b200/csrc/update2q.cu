@@ -1439,14 +1439,10 @@ static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb
     // quads and a round has at most that many quad tasks per slot pair, so
     // 128 threads (64 at chi_cap <= 16) keep every warp busy and let two or
     // more clusters share an SM pair; the tensor-core readout of the mixed
-    // form needs whole 128-thread groups (one warp per TMEM lane quarter).
-    if (mixed) {
-        if (rpl == 1)
-            rc = launch_rpl<1, 128, true>(p, smem, stream);
-        else if (rpl == 2)
-            rc = launch_rpl<2, 128, true>(p, smem, stream);
-        else
-            rc = launch_rpl<4, kUpdThreads, true>(p, smem, stream);
+    // form (chi_cap > 32 only) needs whole 128-thread groups (one warp per
+    // TMEM lane quarter).
+    if (mixed) {  // rpl == 4 here: smaller caps run the FP64 contraction (above)
+        rc = launch_rpl<4, kUpdThreads, true>(p, smem, stream);
     } else {
         if (rpl == 1)
             rc = launch_rpl<1, 64, false>(p, smem, stream);
