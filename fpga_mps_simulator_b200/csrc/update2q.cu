@@ -234,7 +234,11 @@ __device__ __forceinline__ void bcast_rots(const Rot &mine, int lane, Rot &q0, R
 // a' = a - t|g|, b' = b + t|g| and are recomputed from the data only when one
 // of them cancels (below 1e-8 of its old value), decided by one warp vote so
 // that the column reductions stay off the common path (a select would
-// evaluate them after every rotation).
+// evaluate them after every rotation).  The vote's branch also bounds how far
+// the compiler overlaps consecutive rotations: at 128 rows every branch-free
+// form measured (norm checks deferred to the end of a quad round, or exact
+// norms reduced with the inner products) was faster in isolation but spilled
+// in the kernel and ran 1.8-2.7x slower.
 template <int RPL>
 __device__ __forceinline__ int apply_two(double2 (&x0)[RPL], double2 (&y0)[RPL], double &a0, double &b0,
                                          double2 (&x1)[RPL], double2 (&y1)[RPL], double &a1, double &b1,
@@ -527,9 +531,10 @@ __device__ void exchange_slots(cg::cluster_group &cluster, const Slots &S, doubl
 // ------------------------------------------------------ QR preconditioner
 // One-sided Jacobi converges in far fewer sweeps on R^H, R the triangular
 // factor of a QR of X with columns in decreasing norm order, than on X
-// itself (the preconditioner of Drmac and Veselic; measured on the
-// circuits' theta: 17 -> 8 sweeps on CZ-ansatz layers, 11.4 -> 9 on random
-// brickwork).  X P = Q R with P the sort permutation gives X^H = P R^H Q^H,
+// itself (the preconditioner of Drmac and Veselic; a row-cyclic CPU
+// emulation on the theta of these circuits: 17 -> 8 sweeps for CZ-ansatz
+// layers, 11.4 -> 9 for random brickwork; the kernel, timed: 17.6 -> 11.5
+// and 11.5 -> 9.9).  X P = Q R with P the sort permutation gives X^H = P R^H Q^H,
 // so the Jacobi on Z = R^H yields X's right singular vectors (rows permuted
 // by P) times S, and the left ones follow as U S^2 = X0 P Z_k from the
 // unrotated copy X0, the same projection the unpreconditioned path uses on
