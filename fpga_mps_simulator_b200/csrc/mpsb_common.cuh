@@ -73,10 +73,11 @@ struct PairRec {
 //                QR-preconditioned factorisation) v_k S_k at
 //                [Q + k C, Q + (k + 1) C)
 //   [2Q, 2Q+72)  144 doubles: S[0..128), then keep, the kept-norm divisor,
-//                R, C and the side flag
+//                R, C, the side flag and the number of Jacobi sweeps
 // rounded up to a multiple of 16 double2 (256 bytes).
 constexpr int kTapeMetaKeep = 128, kTapeMetaDiv = 129, kTapeMetaRows = 130, kTapeMetaCols = 131;
 constexpr int kTapeMetaSide = 132;
+constexpr int kTapeMetaSweeps = 133;  // Jacobi sweeps taken (the final one without rotations included)
 __host__ __device__ inline long long tape_stride(int chi_cap) {
     const long long q = (long long)(2 * chi_cap) * (2 * chi_cap);
     return (2 * q + 72 + 15) & ~15LL;

@@ -1095,7 +1095,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
     int parity = 0;
     int tmo = 0;
     bool converged = false;
+    int sweeps = 0;
     for (int sweep = 0; sweep < p.max_sweeps; ++sweep) {
+        sweeps = sweep + 1;
         const int sb = sweep & 1;
         if (tid == 0) sc->nrot[sb] = 0;
         recompute_norms<RPL, NT>(S, w, warp, lane);
@@ -1345,6 +1347,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
                 meta[kTapeMetaRows] = (double)R;
                 meta[kTapeMetaCols] = (double)C;
                 meta[kTapeMetaSide] = precond ? 1.0 : 0.0;
+                meta[kTapeMetaSweeps] = (double)sweeps;
             }
         }
     }
