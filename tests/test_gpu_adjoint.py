@@ -52,6 +52,9 @@ def _get(t, b, k, shape):
     (32, 32, 32, 32, 1e-12, "general", True),
     (64, 64, 64, 64, 1e-10, "haar", True),
     (12, 16, 24, 32, 1e-12, "haar", True),    # wide: preconditioned Jacobi on theta^H
+    (20, 16, 13, 32, 1e-12, "haar", True),    # tall, C = 26: the last QR panel half padding
+    (24, 24, 24, 32, 1e-12, "haar", True),    # C_pad = 48: two quads on some warps, one on others
+    (40, 32, 45, 64, 1e-12, "general", True),  # wide, C = 80 at chi_cap 64
     (4, 8, 4, 64, 1e-12, "haar", True),       # too few columns for the preconditioner
 ])
 def test_update_backward_matches_oracle(cl, cm, cr, chi, cut, gate_kind, graded):
