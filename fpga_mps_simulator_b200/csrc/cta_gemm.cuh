@@ -15,8 +15,19 @@ struct GemmSmem {
     double2 b[kGK][kGT + 1];
 };
 
+// FP64 tensor-core MMA (the sm_80+ mma.sync shape; tcgen05 has no FP64
+// kind): D = A B + D for an 8 x 8 block, k = 4.  Fragments: a = A[g][t4],
+// b = B[t4][g], d = D[g][2 t4 + {0, 1}] with g = lane / 4, t4 = lane % 4.
+__device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
 // out(i, j, sum_k a(i, k) b(k, j)) for i < m, j < n, k < kk, by all 256
-// threads of the CTA (each owns 4 x 4 outputs of a 64 x 64 tile).  AK / BJ
+// threads of the CTA: warp w owns rows 8w..8w+7 of a 64 x 64 tile, as eight
+// 8 x 8 blocks computed with FP64 tensor-core MMAs (a complex k4 step is four
+// real MMAs: Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br).  AK / BJ
 // choose which index runs fastest across threads while a tile is staged, so
 // that row-major and transposed operands both load contiguously.  The next
 // k chunk's operands are fetched into registers while the current chunk
@@ -25,7 +36,7 @@ struct GemmSmem {
 template <bool AK, bool BJ, class FA, class FB, class FO>
 __device__ void cta_cgemm(int m, int n, int kk, FA fa, FB fb, FO out, GemmSmem &sm) {
     constexpr int kPer = kGK * kGT / kCtaGemmThreads;  // elements of each operand per thread and chunk
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
     auto a_at = [&](int q, int &ii, int &kq) {
         const int e = tid + q * kCtaGemmThreads;
         if (AK) {
@@ -48,11 +59,9 @@ __device__ void cta_cgemm(int m, int n, int kk, FA fa, FB fb, FO out, GemmSmem &
     };
     for (int i0 = 0; i0 < m; i0 += kGT) {
         for (int j0 = 0; j0 < n; j0 += kGT) {
-            double2 acc[4][4];
+            double cr[8][2], ci[8][2];  // warp's 8 x 64 strip: 8 blocks of 8 x 8, real and imaginary
 #pragma unroll
-            for (int qi = 0; qi < 4; ++qi)
-#pragma unroll
-                for (int qj = 0; qj < 4; ++qj) acc[qi][qj] = make_double2(0.0, 0.0);
+            for (int cb = 0; cb < 8; ++cb) cr[cb][0] = cr[cb][1] = ci[cb][0] = ci[cb][1] = 0.0;
             double2 ra[kPer], rb[kPer];
             auto fetch = [&](int k0) {
 #pragma unroll
@@ -78,26 +87,27 @@ __device__ void cta_cgemm(int m, int n, int kk, FA fa, FB fb, FO out, GemmSmem &
                 }
                 __syncthreads();
                 if (k0 + kGK < kk) fetch(k0 + kGK);
-#pragma unroll 4
-                for (int kq = 0; kq < kGK; ++kq) {
-                    double2 av[4], bv[4];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        av[q] = sm.a[kq][ty + 16 * q];
-                        bv[q] = sm.b[kq][tx + 16 * q];
+                for (int k4 = 0; k4 < kGK; k4 += 4) {
+                    const double2 av = sm.a[k4 + t4][8 * warp + g];
+                    const double nai = -av.y;
+#pragma unroll
+                    for (int cb = 0; cb < 8; ++cb) {
+                        const double2 bv = sm.b[k4 + t4][8 * cb + g];
+                        dmma_m8n8k4(cr[cb][0], cr[cb][1], av.x, bv.x);
+                        dmma_m8n8k4(cr[cb][0], cr[cb][1], nai, bv.y);
+                        dmma_m8n8k4(ci[cb][0], ci[cb][1], av.x, bv.y);
+                        dmma_m8n8k4(ci[cb][0], ci[cb][1], av.y, bv.x);
                     }
-#pragma unroll
-                    for (int qi = 0; qi < 4; ++qi)
-#pragma unroll
-                        for (int qj = 0; qj < 4; ++qj) acc[qi][qj] = c_fma(av[qi], bv[qj], acc[qi][qj]);
                 }
             }
+            const int i = i0 + 8 * warp + g;
 #pragma unroll
-            for (int qi = 0; qi < 4; ++qi)
+            for (int cb = 0; cb < 8; ++cb)
 #pragma unroll
-                for (int qj = 0; qj < 4; ++qj) {
-                    const int i = i0 + ty + 16 * qi, j = j0 + tx + 16 * qj;
-                    if (i < m && j < n) out(i, j, acc[qi][qj]);
+                for (int h = 0; h < 2; ++h) {
+                    const int j = j0 + 8 * cb + 2 * t4 + h;
+                    if (i < m && j < n) out(i, j, make_double2(cr[cb][h], ci[cb][h]));
                 }
         }
     }
