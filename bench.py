@@ -547,9 +547,10 @@ def run_ours(args) -> None:
         flops = sum(update_flops(cl, cm, cr) for per in dims for cl, cm, cr, _ in per)
         hbm = sum(update_bytes(cl, cm, cr, k) for per in dims for cl, cm, cr, k in per)
         kern_s = layer_ms.sum() * 1e-3 / args.steps
+        trunc = np.concatenate([pb.trunc.cpu().numpy() for pb in pbs])  # discarded weight per update
         return {"batch": batch, "value": world * n_upd * args.steps / total_s, "total_s": total_s,
                 "flops": flops, "hbm": hbm, "kern_s": kern_s, "clocks": clk,
-                "achieved_tf": flops / kern_s / 1e12}
+                "achieved_tf": flops / kern_s / 1e12, "trunc": trunc}
 
     main = measure(precision, timed=True)
     other_prec = "fp64" if precision == "mixed" else "mixed"
@@ -562,6 +563,16 @@ def run_ours(args) -> None:
     bb, lbb = overlap(other["batch"], 0, other["batch"], 0)
     infid = 1.0 - abs(ab) ** 2 / (aa.real * bb.real) * math.exp(2 * lab - laa - lbb)
     batch = main["batch"]
+    # per-update truncation error (discarded weight) of both forms, and <Z_i> on every site
+    zop = np.diag([1.0, -1.0]).astype(np.complex128)
+    zterms = [(i, zop, None) for i in range(N_SITES)]
+    z_main = main["batch"].expect_terms(zterms)[0]
+    z_other = other["batch"].expect_terms(zterms)[0]
+    tr_m, tr_o = main["trunc"], other["trunc"]
+    form_errors = {"discarded_weight_per_update": {f"{precision}_mean": float(tr_m.mean()),
+                                                   f"{other_prec}_mean": float(tr_o.mean()),
+                                                   "max_abs_diff": float(np.max(np.abs(tr_m - tr_o)))},
+                   "z_expectation_max_abs_diff": float(np.max(np.abs(z_main - z_other)))}
 
     # ---- per-update drop-in path (FP64, one update per call, no batching), one saturated layer
     single = None
@@ -635,7 +646,7 @@ def run_ours(args) -> None:
         "warmup": args.warmup, "ms_per_step": round(total_s * 1e3 / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f64+tf32x3",
         "forms": {precision: round(value, 3), other_prec: round(other["value"], 3),
-                  "infidelity_mixed_vs_fp64": infid,
+                  "infidelity_mixed_vs_fp64": infid, **form_errors,
                   "note": "batched per layer; mixed = 3xTF32 tcgen05 complex-3M theta + FP64 Jacobi SVD"},
         "data": "synthetic (seeded Haar-random 4x4 gates, |0...0> start)",
         "config": {"workload": WORKLOAD, "precision": precision, "updates_per_step": n_upd,
