@@ -637,6 +637,8 @@ def run_ours(args) -> None:
         from oracle.cpu_baseline import usable_cores
         cw = usable_cores() if (rank == 0 and world == 1 and not args.no_cpu) else 0
         gradient = gradient_leg(dev, 5, 3, rank, max_over_ranks, cpu_workers=cw)
+        for key in ("fp64", "mixed", "fp64_checkpointed"):  # fraction of the same FP64 roofline
+            gradient[key]["roofline_frac"] = round(gradient[key]["achieved_tflops"] / fp64_peak_tflops, 4)
 
     reps.close()
     if rank != 0:
