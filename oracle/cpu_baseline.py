@@ -46,6 +46,8 @@ def _worker(args) -> Tuple[int, float]:
     if here not in sys.path:
         sys.path.insert(0, here)
     from oracle.mps_oracle import OracleMPS
+    if limiter is not None:  # again, now that scipy's BLAS is loaded too
+        limiter = threadpool_limits(1)
     gates = _circuit(n, depth, seed)
     t0 = time.perf_counter()
     count = 0
@@ -71,7 +73,7 @@ def run_parallel(n: int, depth: int, chi: int, cutoff: float, workers: int, reps
     """Aggregate updates/s of `workers` single-threaded processes, each running `reps` circuits."""
     own = pool is None
     if own:
-        pool = mp.get_context("spawn").Pool(workers)
+        pool = _single_thread_pool(workers)
     try:
         t0 = time.perf_counter()
         res = pool.map(_worker, [(n, depth, chi, cutoff, seed + w, reps) for w in range(workers)])
@@ -85,8 +87,31 @@ def run_parallel(n: int, depth: int, chi: int, cutoff: float, workers: int, reps
             "per_worker_s": float(np.mean([r[1] for r in res])), "workers": workers}
 
 
+_SINGLE_THREAD_ENV = ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS", "BLIS_NUM_THREADS")
+
+
+def _single_thread_pool(workers: int):
+    """Spawn pool whose workers start with every BLAS thread pool at one thread.
+    The variables are read when each BLAS library loads, whatever order a
+    worker imports numpy and scipy in; the runtime limit inside the workers
+    reaches only libraries already loaded, and scipy's own OpenBLAS loading
+    after it left 8 workers x 8 spinning threads on an 8-core host.  The
+    parent's environment is restored once the workers exist."""
+    saved = {k: os.environ.get(k) for k in _SINGLE_THREAD_ENV}
+    try:
+        for k in _SINGLE_THREAD_ENV:
+            os.environ[k] = "1"
+        return mp.get_context("spawn").Pool(workers)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
 def make_pool(workers: int):
-    return mp.get_context("spawn").Pool(workers)
+    return _single_thread_pool(workers)
 
 
 def _grad_worker(args) -> Tuple[int, float]:
@@ -101,6 +126,8 @@ def _grad_worker(args) -> Tuple[int, float]:
     if here not in sys.path:
         sys.path.insert(0, here)
     from oracle.mps_adjoint import hea_energy_grad, tfim_mpo
+    if limiter is not None:  # again, now that scipy's BLAS is loaded too
+        limiter = threadpool_limits(1)
     rng = np.random.default_rng(seed)
     angles = rng.uniform(0.0, 2.0 * math.pi, size=(layers, n, 2))
     t0 = time.perf_counter()
@@ -116,7 +143,7 @@ def run_grad_parallel(n: int, layers: int, chi: int, cutoff: float, workers: int
     (single BLAS thread each); returns aggregate parameter vectors per second."""
     own = pool is None
     if own:
-        pool = mp.get_context("spawn").Pool(workers)
+        pool = _single_thread_pool(workers)
     try:
         t0 = time.perf_counter()
         res = pool.map(_grad_worker, [(n, layers, chi, cutoff, seed + w) for w in range(workers)])
@@ -142,6 +169,8 @@ def _fwd_worker(args) -> Tuple[int, float]:
     if here not in sys.path:
         sys.path.insert(0, here)
     from oracle.mps_adjoint import hea_energy, tfim_mpo
+    if limiter is not None:  # again, now that scipy's BLAS is loaded too
+        limiter = threadpool_limits(1)
     rng = np.random.default_rng(seed)
     angles = rng.uniform(0.0, 2.0 * math.pi, size=(layers, n, 2))
     t0 = time.perf_counter()
@@ -157,7 +186,7 @@ def run_forward_parallel(n: int, layers: int, chi: int, cutoff: float, workers: 
     gradient) per worker process; returns the mean seconds per evaluation."""
     own = pool is None
     if own:
-        pool = mp.get_context("spawn").Pool(workers)
+        pool = _single_thread_pool(workers)
     try:
         res = pool.map(_fwd_worker, [(n, layers, chi, cutoff, seed + w) for w in range(workers)])
     finally:
