@@ -16,7 +16,14 @@ LIB_PATH = os.path.join(_HERE, "libmpsb200.so")
 MPSB_CHI_LIMIT = 64
 FP64 = 0
 MIXED_TF32X3 = 1
-ST_NOCONV, ST_NONFINITE, ST_BADDIM = 1, 2, 4
+ST_NOCONV, ST_NONFINITE, ST_BADDIM, ST_TIMEOUT, ST_CHI_LIMIT = 1, 2, 4, 8, 16
+
+
+def keep_limit(n: int, chi_max: int) -> int:
+    """Largest bond an update of an n-site chain with this chi_max forms on the
+    device: min(chi_max, MPSB_CHI_LIMIT, 2^(n//2)) (the kernels' keep_limit)."""
+    schmidt = 1 << 7 if n >= 14 else (1 if n < 2 else 1 << (n // 2))
+    return min(int(chi_max), MPSB_CHI_LIMIT, schmidt)
 _ERRORS = {-1: "EINVAL", -2: "ELAUNCH", -3: "EWORKSPACE", -4: "ENODEV"}
 
 # Symbols the header declares; tests check that every one is exported.
@@ -97,6 +104,14 @@ def _declare(lib):
         fn.argtypes = args
 
 
+def status_text(st: int) -> str:
+    """Names of the MPSB_ST_* bits set in a status word."""
+    names = [(ST_NOCONV, "Jacobi not converged"), (ST_NONFINITE, "non-finite theta"),
+             (ST_BADDIM, "bad bond dims"), (ST_TIMEOUT, "a bounded wait gave up"),
+             (ST_CHI_LIMIT, f"an update needed a bond above {MPSB_CHI_LIMIT}")]
+    return ", ".join(t for b, t in names if st & b) or "ok"
+
+
 def load(path: str = LIB_PATH):
     """Load (once) and return the library handle."""
     global _lib
@@ -110,6 +125,34 @@ def load(path: str = LIB_PATH):
             _declare(lib)
             _lib = lib
     return _lib
+
+
+class OnDevice:
+    """The library handle with one CUDA device made current around every call.
+
+    Every entry point launches on the current device (and refuses a chain
+    table that lives on another one), so objects that own device memory call
+    through this wrapper rather than the bare handle: a batch built on cuda:1
+    then works whatever device the caller has current.
+    """
+
+    def __init__(self, lib, device):
+        self._lib = lib
+        self._device = device
+
+    def __getattr__(self, name):
+        fn = getattr(self._lib, name)
+        if not callable(fn):
+            return fn
+        device = self._device
+
+        def call(*args):
+            import torch
+            with torch.cuda.device(device):
+                return fn(*args)
+
+        call.__name__ = name
+        return call
 
 
 def check(rc: int, what: str) -> None:

@@ -76,7 +76,7 @@ class AdjointEngine:
         if len(set(batch.ns)) != 1:
             raise ValueError("the energy gradient needs chains of equal length")
         self.b = batch
-        self.lib = _lib.load()
+        self.lib = _lib.OnDevice(_lib.load(), batch.device)
         self.n = batch.ns[0]
         W = check_mpo(mpo, self.n)
         self.D = W.shape[1]

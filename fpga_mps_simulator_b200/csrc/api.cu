@@ -4,6 +4,9 @@
 
 #include <cstdarg>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <utility>
 
 namespace mpsb {
 
@@ -23,12 +26,51 @@ int check_launch(const char *what) {
     return MPSB_OK;
 }
 
-static int check_device() {
+// The current device must be an sm_100 part, and the chain table (when
+// given) must be device memory of that device: every kernel launches on the
+// current device, so a table on another GPU would be read through a wrong
+// address space rather than refused.
+int check_device(const void *table, void *stream) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return set_error(MPSB_ENODEV, "no CUDA device");
     int major = 0;
     cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
     if (major != 10) return set_error(MPSB_ENODEV, "device %d has compute capability %d.x; sm_100 required", dev, major);
+    // (skipped while the stream is being captured into a graph, where only
+    // stream-ordered work belongs)
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (table && cudaStreamIsCapturing(reinterpret_cast<cudaStream_t>(stream), &cap) == cudaSuccess &&
+        cap == cudaStreamCaptureStatusNone) {
+        cudaPointerAttributes at{};
+        const cudaError_t e = cudaPointerGetAttributes(&at, table);
+        if (e != cudaSuccess) {
+            cudaGetLastError();  // clear the error this query leaves behind
+            return set_error(MPSB_EINVAL, "chain table %p is not a CUDA pointer (%s)", table, cudaGetErrorString(e));
+        }
+        if (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)
+            return set_error(MPSB_EINVAL, "chain table %p is not device memory", table);
+        if (at.device != dev)
+            return set_error(MPSB_ENODEV, "chain table lives on device %d but device %d is current", at.device, dev);
+    }
+    return MPSB_OK;
+}
+
+// The dynamic shared-memory limit is a per-device attribute of a kernel, so
+// the largest size enabled so far is remembered per (kernel, device), under a
+// lock (host threads may launch concurrently).  Called before each launch;
+// only a size above the remembered one reaches cudaFuncSetAttribute.
+int ensure_smem(const void *kernel, size_t bytes, const char *what) {
+    if (bytes <= 48 * 1024) return MPSB_OK;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_error(MPSB_ENODEV, "no CUDA device");
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> enabled;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &have = enabled[std::make_pair(kernel, dev)];
+    if (bytes <= have) return MPSB_OK;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+        return check_launch(what);
+    have = bytes;
     return MPSB_OK;
 }
 
@@ -104,7 +146,7 @@ int mpsb_update2q_batch(const mpsb_chain *chains, const mpsb_pair *pairs, int np
         return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
     if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
         return set_error(MPSB_EINVAL, "workspace must be 256-byte aligned");
-    int rc = check_device();
+    int rc = check_device(chains, stream);
     if (rc) return rc;
     if (max_sweeps <= 0) max_sweeps = 40;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
@@ -126,7 +168,7 @@ int mpsb_apply1q_batch(const mpsb_chain *chains, const mpsb_site_op *ops, int no
     if (!chains || !ops || !gates) return set_error(MPSB_EINVAL, "null chains/ops/gates pointer");
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    int rc = check_device();
+    int rc = check_device(chains, stream);
     if (rc) return rc;
     return launch_apply1q(chains, ops, nops, reinterpret_cast<const double2 *>(gates), chi_cap,
                           reinterpret_cast<cudaStream_t>(stream));
@@ -138,7 +180,7 @@ int mpsb_statevector(const mpsb_chain *chain_dev, int n, int chi_cap, mpsb_c128 
     if (n < 1 || n > 24) return set_error(MPSB_EINVAL, "statevector needs 1 <= n <= 24, got %d", n);
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    int rc = check_device();
+    int rc = check_device(chain_dev, stream);
     if (rc) return rc;
     return launch_statevector(chain_dev, n, chi_cap, reinterpret_cast<double2 *>(out),
                               reinterpret_cast<double2 *>(scratch), scratch_bytes,
@@ -151,7 +193,7 @@ int mpsb_amplitude(const mpsb_chain *chains, int chain, int n, const uint8_t *bi
     if (nbits < 0 || n < 1 || chain < 0) return set_error(MPSB_EINVAL, "bad nbits/n/chain");
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    int rc = check_device();
+    int rc = check_device(chains, stream);
     if (rc) return rc;
     return launch_amplitude(chains, chain, n, bits, nbits, reinterpret_cast<double2 *>(out), log_abs,
                             reinterpret_cast<cudaStream_t>(stream));
@@ -175,7 +217,7 @@ int mpsb_expect_local(const mpsb_chain *chains, int nchains, int n, int chi_cap,
     const size_t need = expect_workspace_bytes(nchains, n, chi_cap, nctas);
     if (workspace_bytes < need)
         return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
-    int rc = check_device();
+    int rc = check_device(chains, stream);
     if (rc) return rc;
     return launch_expect(chains, nchains, n, chi_cap, sites, two_site, reinterpret_cast<const double2 *>(ops),
                          nterms, out, workspace, nctas, reinterpret_cast<cudaStream_t>(stream));
@@ -190,7 +232,7 @@ int mpsb_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap, m
     const size_t need = 2 * (size_t)chi_cap * chi_cap * sizeof(double2);
     if (workspace_bytes < need)
         return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
-    int rc = check_device();
+    int rc = check_device(a, stream);
     if (rc) return rc;
     return launch_overlap(a, b, n, chi_cap, reinterpret_cast<double2 *>(out), out_log, workspace,
                           reinterpret_cast<cudaStream_t>(stream));
@@ -211,7 +253,7 @@ int mpsb_sample(const mpsb_chain *chains, int chain, int n, int chi_cap, const d
     const size_t need = sample_workspace_bytes(n, chi_cap);
     if (workspace_bytes < need)
         return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
-    int rc = check_device();
+    int rc = check_device(chains, stream);
     if (rc) return rc;
     return launch_sample(chains, chain, n, chi_cap, uniforms, shots, bits, workspace,
                          reinterpret_cast<cudaStream_t>(stream));
@@ -224,7 +266,7 @@ int mpsb_reset_batch(const mpsb_chain *chains, const mpsb_site_op *ops, int nops
     if (!chains || !ops) return set_error(MPSB_EINVAL, "null chains/ops pointer");
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    int rc = check_device();
+    int rc = check_device(chains, stream);
     if (rc) return rc;
     return launch_reset(chains, ops, nops, reinterpret_cast<cudaStream_t>(stream));
 }
@@ -246,7 +288,7 @@ int mpsb_canonicalize(const mpsb_chain *chains, const int32_t *chain_ids, int nc
     const size_t need = canon_workspace_bytes(nchains, chi_cap);
     if (workspace_bytes < need)
         return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
-    int rc = check_device();
+    int rc = check_device(chains, stream);
     if (rc) return rc;
     return launch_canonicalize(chains, chain_ids, nchains, lo, hi, direction, chi_cap, workspace,
                                reinterpret_cast<cudaStream_t>(stream));
@@ -276,7 +318,7 @@ int mpsb_update2q_batch_taped(const mpsb_chain *chains, const mpsb_pair *pairs, 
     if (tape_bytes < tneed) return set_error(MPSB_EWORKSPACE, "tape of %zu bytes < %zu needed", tape_bytes, tneed);
     if (((reinterpret_cast<uintptr_t>(workspace) | reinterpret_cast<uintptr_t>(tape)) & 255) != 0)
         return set_error(MPSB_EINVAL, "workspace and tape must be 256-byte aligned");
-    int rc = check_device();
+    int rc = check_device(chains, stream);
     if (rc) return rc;
     if (max_sweeps <= 0) max_sweeps = 40;
     const bool mixed = precision == MPSB_MIXED_TF32X3;
@@ -306,7 +348,7 @@ int mpsb_update2q_backward_batch(const mpsb_chain *pre, const mpsb_chain *cot, c
     const size_t need = bwd_workspace_bytes(npairs, chi_cap);
     if (workspace_bytes < need)
         return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
-    int rc = check_device();
+    int rc = check_device(pre, stream);
     if (rc) return rc;
     return launch_update2q_backward(pre, cot, pairs, npairs, reinterpret_cast<const double2 *>(gates), chi_cap, tape,
                                     reinterpret_cast<double2 *>(gate_grads), workspace, status, 1.0e-6, 1.0e-12,
@@ -320,7 +362,7 @@ int mpsb_apply1q_backward_batch(const mpsb_chain *pre, const mpsb_chain *cot, co
     if (!pre || !cot || !ops || !gates) return set_error(MPSB_EINVAL, "null pre/cot/ops/gates pointer");
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    int rc = check_device();
+    int rc = check_device(pre, stream);
     if (rc) return rc;
     return launch_apply1q_backward(pre, cot, ops, nops, reinterpret_cast<const double2 *>(gates),
                                    reinterpret_cast<double2 *>(gate_grads), reinterpret_cast<cudaStream_t>(stream));
@@ -343,7 +385,7 @@ int mpsb_mpo_energy_grad(const mpsb_chain *chains, int nchains, int n, int chi_c
     const size_t need = mpo_grad_workspace_bytes(nchains, n, chi_cap, mpo_bond);
     if (workspace_bytes < need)
         return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
-    int rc = check_device();
+    int rc = check_device(chains, stream);
     if (rc) return rc;
     return launch_mpo_energy_grad(chains, nchains, n, chi_cap, reinterpret_cast<const double2 *>(mpo), mpo_bond,
                                   weights, loss, cot, workspace, reinterpret_cast<cudaStream_t>(stream));
@@ -352,7 +394,7 @@ int mpsb_mpo_energy_grad(const mpsb_chain *chains, int nchains, int n, int chi_c
 int mpsb_fp64_probe(int64_t iters, int blocks, int threads, double *sink, mpsb_stream_t stream) {
     if (iters < 1 || blocks < 1 || threads < 32 || threads > 1024 || !sink)
         return set_error(MPSB_EINVAL, "bad probe arguments");
-    int rc = check_device();
+    int rc = check_device(nullptr, stream);
     if (rc) return rc;
     return launch_fp64_probe(iters, blocks, threads, sink, reinterpret_cast<cudaStream_t>(stream));
 }

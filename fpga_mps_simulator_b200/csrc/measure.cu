@@ -401,13 +401,9 @@ size_t canon_workspace_bytes(int nchains, int chi_cap) {
 int launch_canonicalize(const mpsb_chain *chains, const int32_t *ids, int nchains, int lo, int hi, int dir,
                         int chi_cap, void *ws, cudaStream_t s) {
     if (nchains == 0 || hi < lo) return MPSB_OK;
-    static size_t configured = 0;
     const size_t smem = canon_smem_bytes(chi_cap);
-    if (smem > configured) {
-        if (cudaFuncSetAttribute(canon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return check_launch("cudaFuncSetAttribute(canon)");
-        configured = smem;
-    }
+    const int rc = ensure_smem(reinterpret_cast<const void *>(canon_kernel), smem, "cudaFuncSetAttribute(canon)");
+    if (rc) return rc;
     canon_kernel<<<nchains, kQrThreads, smem, s>>>(chains, ids, lo, hi, dir, chi_cap,
                                                    reinterpret_cast<double2 *>(ws));
     return check_launch("canon_kernel");

@@ -54,6 +54,15 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// Largest bond a two-site update of this chain may form: its chi_max, the
+// device limit MPSB_CHI_LIMIT and the Schmidt-rank bound 2^(n/2) of the
+// middle cut (no bond of an n-site chain can exceed it).
+__host__ __device__ inline int keep_limit(const mpsb_chain &ch) {
+    const int schmidt = ch.n >= 14 ? (1 << 7) : (ch.n < 2 ? 1 : (1 << (ch.n / 2)));
+    int k = ch.chi_max < MPSB_CHI_LIMIT ? ch.chi_max : MPSB_CHI_LIMIT;
+    return k < schmidt ? k : schmidt;
+}
+
 // Per-pair bookkeeping written by the update kernel, folded into norm_log by
 // a second kernel in pair order.
 struct PairRec {
@@ -89,4 +98,6 @@ __host__ __device__ inline long long tape_stride(int chi_cap) {
 namespace mpsb {
 int set_error(int code, const char *fmt, ...);
 int check_launch(const char *what);
+int check_device(const void *table, void *stream);
+int ensure_smem(const void *kernel, size_t bytes, const char *what);
 }  // namespace mpsb

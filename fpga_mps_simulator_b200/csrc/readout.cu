@@ -388,15 +388,11 @@ int launch_expect(const mpsb_chain *chains, int nchains, int n, int chi_cap, con
     double2 *tscr = envR + (size_t)nchains * (n + 1) * es;
     double2 *cscr = tscr + (size_t)nchains * 2 * es;
     const size_t smem_env = 2 * es * sizeof(double2);
-    static size_t configured_env = 0;
-    if (configured_env < smem_env) {
-        if (cudaFuncSetAttribute(environments_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_env) !=
-            cudaSuccess)
-            return check_launch("cudaFuncSetAttribute(environments)");
-        configured_env = smem_env;
-    }
+    int rc = ensure_smem(reinterpret_cast<const void *>(environments_kernel), smem_env,
+                         "cudaFuncSetAttribute(environments)");
+    if (rc) return rc;
     environments_kernel<<<nchains, 256, smem_env, s>>>(chains, n, chi_cap, envL, envR, tscr);
-    int rc = check_launch("environments_kernel");
+    rc = check_launch("environments_kernel");
     if (rc) return rc;
     const int grid = nchains * nterms < nctas ? nchains * nterms : nctas;
     terms_kernel<<<grid, 256, 0, s>>>(chains, nchains, n, chi_cap, envL, envR, sites, two_site, ops, nterms, out,
@@ -460,13 +456,8 @@ __global__ void __launch_bounds__(kCtaGemmThreads, 1)
 int launch_overlap(const mpsb_chain *a, const mpsb_chain *b, int n, int chi_cap, double2 *out, double *out_log,
                    void *ws, cudaStream_t s) {
     const size_t smem = 2 * (size_t)chi_cap * chi_cap * sizeof(double2);
-    static size_t configured = 0;
-    if (smem > configured) {
-        if (cudaFuncSetAttribute(overlap_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-            return check_launch("cudaFuncSetAttribute(overlap)");
-        configured = smem;
-    }
+    const int rc = ensure_smem(reinterpret_cast<const void *>(overlap_kernel), smem, "cudaFuncSetAttribute(overlap)");
+    if (rc) return rc;
     overlap_kernel<<<1, kCtaGemmThreads, smem, s>>>(a, b, n, chi_cap, out, out_log, reinterpret_cast<double2 *>(ws));
     return check_launch("overlap_kernel");
 }

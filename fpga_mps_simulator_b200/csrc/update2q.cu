@@ -974,7 +974,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
         cm = ch.bonds[i + 1];
         cr = ch.bonds[i + 2];
         bad = cl < 1 || cm < 1 || cr < 1 || cl > p.chi_cap || cm > p.chi_cap || cr > p.chi_cap ||
-              ch.chi_max < 1 || ch.chi_max > p.chi_cap;
+              ch.chi_max < 1 || keep_limit(ch) > p.chi_cap;
     }
     if (bad) {  // both CTAs see the same data and leave together
         if (crank == 0 && tid == 0) {
@@ -1171,7 +1171,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
             cnt += (v > thr);
             tot = fma(v, v, tot);
         }
-        const int keep = min(max(cnt, 1), ch.chi_max);
+        // the reference's rule keeps min(max(cnt, 1), chi_max); bonds above
+        // MPSB_CHI_LIMIT are never formed, and a pair that would need one keeps
+        // the limit and says so (MPSB_ST_CHI_LIMIT)
+        const int wanted = min(max(cnt, 1), ch.chi_max);
+        const int keep = min(wanted, keep_limit(ch));
         double dropped = 0.0;
         for (int k = keep; k < C; ++k) dropped = fma(Ssorted[k], Ssorted[k], dropped);
         double d1 = 0.0;
@@ -1192,6 +1196,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
         sc->nk = nk;
         if (crank == 0) {
             int st = converged ? 0 : MPSB_ST_NOCONV;
+            if (wanted > keep) st |= MPSB_ST_CHI_LIMIT;
             if (sc->nonfinite | remote_nonfinite) st |= MPSB_ST_NONFINITE;
             if (sc->timeout | remote_timeout) st |= MPSB_ST_TIMEOUT;
             const double disc = tot > 0.0 ? dropped / tot : 0.0;
@@ -1388,13 +1393,9 @@ size_t upd_workspace_bytes(int npairs, int chi_cap) {
 
 template <int RPL, int NT, bool MIXED>
 static int launch_rpl(const Upd2Params &p, size_t smem, cudaStream_t s) {
-    static size_t configured = 0;  // largest dynamic shared memory size enabled so far
-    if (smem > configured) {
-        if (cudaFuncSetAttribute(update2q_fp64_kernel<RPL, NT, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return check_launch("cudaFuncSetAttribute(update2q)");
-        configured = smem;
-    }
+    const int rc = ensure_smem(reinterpret_cast<const void *>(update2q_fp64_kernel<RPL, NT, MIXED>), smem,
+                               "cudaFuncSetAttribute(update2q)");
+    if (rc) return rc;
     update2q_fp64_kernel<RPL, NT, MIXED><<<2 * p.npairs, NT, smem, s>>>(p);
     return check_launch("update2q kernel");
 }

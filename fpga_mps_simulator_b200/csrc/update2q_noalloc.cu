@@ -15,6 +15,10 @@
 // address is looked up once per device with cudaGetSymbolAddress while that
 // device is current; the first call on a device does this set-up, which is
 // why that first call should come before any stream capture on the device.
+// The address is kept per device ordinal for the life of the process: it
+// assumes the device keeps one primary context throughout.  After a
+// cudaDeviceReset the module is loaded again and the kept address is stale,
+// so this entry must not be used across a device reset.
 // All calls share the one array and it keeps the last call's contents; the
 // kernels write every scratch byte they later read within the same call, so
 // nothing has to be cleared between calls.  Two calls whose kernels overlap
@@ -81,12 +85,10 @@ extern "C" int mpsb_update2q_batch_noalloc(const mpsb_chain *chains, const mpsb_
                          "no-alloc update: %d pairs at chi_cap=%d need %zu scratch bytes, more than the fixed "
                          "%zu; split the batch or use mpsb_update2q_batch with a workspace",
                          npairs, chi_cap, need, (size_t)MPSB_NOALLOC_SCRATCH_BYTES);
-    int dev = 0, major = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return set_error(MPSB_ENODEV, "no CUDA device");
-    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-    if (major != 10) return set_error(MPSB_ENODEV, "device %d has compute capability %d.x; sm_100 required", dev, major);
+    int rc = check_device(chains, stream);
+    if (rc) return rc;
     void *scratch = nullptr;
-    int rc = noalloc_scratch(&scratch);
+    rc = noalloc_scratch(&scratch);
     if (rc) return rc;
     if (max_sweeps <= 0) max_sweeps = 40;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);

@@ -138,7 +138,6 @@ class MPSBatch:
     def __init__(self, ns: Sequence[int], chi_maxs: Union[int, Sequence[int]] = 64,
                  cutoffs: Union[float, Sequence[float]] = 1e-12, precision: str = "fp64",
                  device: Union[str, torch.device] = "cuda", tol: float = 0.0, max_sweeps: int = 0):
-        self._lib = _lib.load()
         ns = [int(v) for v in ns]
         nch = len(ns)
         chi_maxs = [int(chi_maxs)] * nch if np.isscalar(chi_maxs) else [int(v) for v in chi_maxs]
@@ -148,9 +147,8 @@ class MPSBatch:
         for n, chi in zip(ns, chi_maxs):
             if n < 1:
                 raise ValueError(f"chain length must be >= 1, got {n}")
-            if not (1 <= chi <= _lib.MPSB_CHI_LIMIT):
-                raise ValueError(f"chi_max must be in [1, {_lib.MPSB_CHI_LIMIT}], got {chi}: the fused "
-                                 "kernel holds theta (<= 128 x 128) on chip")
+            if chi < 1:
+                raise ValueError(f"chi_max must be >= 1, got {chi}")
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         self.device = torch.device(device)
@@ -158,13 +156,18 @@ class MPSBatch:
             raise ValueError("MPSBatch lives on a CUDA device; there is no CPU engine")
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
+        self._lib = _lib.OnDevice(_lib.load(), self.device)
         self.precision = precision
         self.tol = float(tol)
         self.max_sweeps = int(max_sweeps)
         self.ns = ns
         self.chi_maxs = chi_maxs
         self.cutoffs = cutoffs
-        self.chi_cap = max(chi_maxs)
+        # device bond cap per chain: min(chi_max, MPSB_CHI_LIMIT, 2^(n//2)); a chain
+        # whose chi_max exceeds the limit reports MPSB_ST_CHI_LIMIT from the first
+        # update that would keep more than the limit
+        self.caps = [_lib.keep_limit(n, chi) for n, chi in zip(ns, chi_maxs)]
+        self.chi_cap = max(self.caps)
         self.slot = 2 * self.chi_cap * self.chi_cap
         self.site_off = np.concatenate([[0], np.cumsum(ns)]).astype(np.int64)
         self.bond_off = self.site_off + np.arange(nch + 1)
@@ -280,9 +283,13 @@ class MPSBatch:
     def check_status(self, raise_on_error: bool = True) -> np.ndarray:
         st = self.status_acc.cpu().numpy()
         if raise_on_error and np.any(st):
-            bad = {int(c): int(v) for c, v in enumerate(st) if v}
-            raise RuntimeError(f"two-site update reported numerical faults per chain {bad} "
-                               "(1 = Jacobi not converged, 2 = non-finite theta, 4 = bad bond dims)")
+            bad = {int(c): f"{int(v)} ({_lib.status_text(int(v))})" for c, v in enumerate(st) if v}
+            hint = ""
+            if any(int(v) & _lib.ST_CHI_LIMIT for v in st):
+                hint = (f"; this device path forms bonds of at most {_lib.MPSB_CHI_LIMIT}, so an update whose "
+                        f"chi_max allows more cannot follow mps_core: pass chi_max <= {_lib.MPSB_CHI_LIMIT} to "
+                        "truncate there")
+            raise RuntimeError(f"two-site update reported faults per chain {bad}{hint}")
         return st
 
     def bond_dims(self, c: int = 0) -> List[int]:
@@ -307,6 +314,8 @@ class MPSBatch:
             raise ValueError("boundary bonds must be 1")
         if max(t.shape[0], t.shape[2]) > self.chi_maxs[c]:
             raise ValueError("bond dimension above chi_max")
+        if max(t.shape[0], t.shape[2]) > self.caps[c]:
+            raise ValueError(f"bond dimension above the device limit {self.caps[c]}")
         # a bond can never exceed the Schmidt rank bound 2^min(left sites, right sites)
         if t.shape[0] > 2 ** min(k, n - k) or t.shape[2] > 2 ** min(k + 1, n - k - 1):
             raise ValueError("bond dimension above the Schmidt-rank bound of its cut")
@@ -482,13 +491,19 @@ class _SitesView:
 class MPSState:
     """One MPS chain on the GPU with the reference class's interface.
 
-    Parameters follow mps_core.MPSState(n, chi_max, svd_cutoff); ``chi_max``
-    is capped at 64 (the FPGA build of the reference caps it the same way,
-    fpga_mps_simulator.py:80-85).  ``precision`` selects the FP64 drop-in form
-    or the mixed 3xTF32 form.
+    Parameters follow mps_core.MPSState(n, chi_max=256, svd_cutoff=1e-12)
+    (mps_core.py:185), defaults included.  The device forms bonds of at most
+    64 (theta <= 128 x 128 on chip; the reference's FPGA build caps chi the
+    same way, fpga_mps_simulator.py:80-85).  Any chi_max is accepted: while no
+    update would keep more than 64 values -- always for n <= 12, where no
+    bond can exceed 64 -- the state follows mps_core exactly; an update that
+    would keep more marks the chain (status MPSB_ST_CHI_LIMIT) and every
+    read-out then raises instead of returning a state that differs from the
+    reference's.  ``precision`` selects the FP64 drop-in form or the mixed
+    3xTF32 form.
     """
 
-    def __init__(self, n: int, chi_max: int = 64, svd_cutoff: float = 1e-12, precision: str = "fp64",
+    def __init__(self, n: int, chi_max: int = 256, svd_cutoff: float = 1e-12, precision: str = "fp64",
                  device: Union[str, torch.device] = "cuda", tol: float = 0.0, max_sweeps: int = 0):
         self.n = int(n)
         self.chi_max = int(chi_max)
@@ -641,10 +656,65 @@ class MPSState:
         s = s / np.linalg.norm(s)
         return s[s > 1e-15]
 
-    def entanglement_entropy(self, bond: int) -> float:
-        """von Neumann entropy -sum p log p, p = Schmidt coefficients squared, at the cut after site ``bond``
-        (the quantity of mps_core.py:465-483, exact in any gauge)."""
+    def exact_entanglement_entropy(self, bond: int) -> float:
+        """von Neumann entropy -sum p log p of the true Schmidt coefficients at the cut
+        after site ``bond`` (``schmidt_values``): exact in any gauge.  The reference's
+        ``entanglement_entropy`` equals it only in mixed-canonical form."""
         p = self.schmidt_values(bond) ** 2
+        return -float(np.sum(p * np.log(np.maximum(p, 1e-300))))
+
+    def _site_matrix_spectrum(self, m: "MPSState", k: int) -> np.ndarray:
+        """Singular values of site k of the scratch copy m read as a (2 chi_l) x chi_r
+        matrix, by the fused update kernel: site k+1 is replaced by a row isometry E
+        (chi_r x 2 chi', E[b, t, c] = 1 where t chi' + c = b, chi' = ceil(chi_r / 2)),
+        so theta = M E has M's singular values, padded with zeros, which the kernel
+        records before truncating.  m is consumed."""
+        b = m._b
+        bonds = b.bonds[: self.n + 1].cpu().numpy()
+        cl, cr = int(bonds[k]), int(bonds[k + 1])
+        if k == self.n - 1:  # a column: its one singular value is its 2-norm
+            return np.array([float(torch.linalg.vector_norm(b.sites[k, : 2 * cl]).item())])
+        cp = (cr + 1) // 2
+        eye = torch.zeros(b.slot, dtype=torch.complex128, device=b.device)
+        rows = torch.arange(cr, device=b.device)
+        eye[rows * (2 * cp) + (rows // cp) * cp + rows % cp] = 1.0  # E[b, b // cp, b % cp] = 1
+        b.sites[k + 1].copy_(eye)
+        b.bonds[k + 2] = cp
+        pb = b.apply_layer([0], [k], np.eye(4, dtype=np.complex128)[None], precision="fp64",
+                           record_spectra=True)
+        s = pb.spectra[0].cpu().numpy()
+        return s[: min(2 * cl, cr)]
+
+    def bond_spectrum(self, bond: int) -> np.ndarray:
+        """Singular values at ``bond`` as mps_core.py:485-494 computes them: on a copy,
+        left-normalise sites 0..bond (QR), then the singular values of site ``bond``
+        as a (2 chi_l) x chi_r matrix -- an isometry after the QR, so ones up to
+        rounding (``schmidt_values`` gives the Schmidt coefficients)."""
+        if not 0 <= bond < self.n:
+            raise ValueError(f"bond {bond} out of range [0, {self.n - 1}]")
+        self.check_status()
+        m = self.copy()
+        m._b.canonicalize([0], 0, bond, "left")
+        return self._site_matrix_spectrum(m, bond)
+
+    def entanglement_entropy(self, bond: int) -> float:
+        """-sum p log p at the bond between sites ``bond`` and ``bond+1`` as
+        mps_core.py:465-483 computes it: p = S^2 / sum S^2 over the singular values
+        S > 1e-15 of the left block (sites 0..bond contracted into a
+        2^(bond+1) x chi matrix).  That is the true entropy only in mixed-canonical
+        form; ``exact_entanglement_entropy`` is exact in any gauge.  The left block
+        is never formed: after left-normalising sites 0..bond-1 of a copy it equals
+        an isometry times site ``bond``, whose singular values the update kernel takes."""
+        if not 0 <= bond < self.n - 1:
+            raise ValueError(f"bond {bond} out of range [0, {self.n - 2}]")
+        self.check_status()
+        m = self.copy()
+        if bond >= 1:
+            m._b.canonicalize([0], 0, bond - 1, "left")
+        s = self._site_matrix_spectrum(m, bond)
+        s = s[s > 1e-15]
+        p = s * s
+        p = p / p.sum()
         return -float(np.sum(p * np.log(np.maximum(p, 1e-300))))
 
     # -- measurement (mps_core.py:354-429) ------------------------------------

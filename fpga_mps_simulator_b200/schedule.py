@@ -66,7 +66,7 @@ class Schedule:
         return sum(len(L.sites) for ls in self.per_chain for L in ls)
 
     def signature(self) -> Tuple:
-        chis = np.asarray(self.batch.chi_maxs)
+        chis = np.asarray(self.batch.caps)
         vals, counts = np.unique(chis, return_counts=True)
         hist = tuple((int(v), int(c)) for v, c in zip(vals, counts))
         return (hist, self.batch.nchains, self.depth, self.updates(), self.batch.precision)
@@ -88,7 +88,7 @@ class Schedule:
             raise ValueError(f"unknown strategy {strategy!r}; choose from {STRATEGIES}")
         b = self.batch
         natural = list(range(b.nchains))
-        by_cost = sorted(natural, key=lambda c: -_cost(b.chi_maxs[c]))
+        by_cost = sorted(natural, key=lambda c: -_cost(b.caps[c]))
         out: List[List[_Launch]] = []
         for L in range(self.depth):
             ls: List[_Launch] = []
@@ -96,10 +96,10 @@ class Schedule:
                 ci, si, gs = self._layer_chains(L, natural if strategy == "single" else by_cost)
                 if ci:
                     ls.append(_Launch(b.make_pairs(ci, si, np.concatenate(gs), self.record_spectra),
-                                      max(b.chi_maxs[c] for c in set(ci))))
+                                      max(b.caps[c] for c in set(ci))))
             else:
-                for cap in sorted(set(b.chi_maxs), reverse=True):
-                    ci, si, gs = self._layer_chains(L, [c for c in natural if b.chi_maxs[c] == cap])
+                for cap in sorted(set(b.caps), reverse=True):
+                    ci, si, gs = self._layer_chains(L, [c for c in natural if b.caps[c] == cap])
                     if ci:
                         ls.append(_Launch(b.make_pairs(ci, si, np.concatenate(gs), self.record_spectra), cap))
             out.append(ls)

@@ -51,9 +51,14 @@ typedef struct {
     int32_t   *bonds;      /* device: n + 1 bond dimensions                      */
     double    *norm_log;   /* device: one double, accumulated log-norm           */
     int32_t   *status_acc; /* device: OR of every pair status of this chain, or NULL */
-    int64_t    slot_elems; /* complex elements per slot, >= 2 * chi_max^2       */
+    int64_t    slot_elems; /* complex elements per slot, >= 2 * chi_cap^2 of every
+                              launch that touches the chain                        */
     int32_t    n;          /* number of sites                                    */
-    int32_t    chi_max;    /* truncation cap, 1 .. MPSB_CHI_LIMIT               */
+    int32_t    chi_max;    /* truncation cap (>= 1; mps_core's default is 256).  No
+                              bond above MPSB_CHI_LIMIT is ever formed: a pair whose
+                              rule would keep more keeps MPSB_CHI_LIMIT values and
+                              reports MPSB_ST_CHI_LIMIT.  The launch's chi_cap must
+                              cover min(chi_max, MPSB_CHI_LIMIT, 2^(n/2)).          */
     double     cutoff;     /* relative singular-value cutoff (svd_cutoff)       */
 } mpsb_chain;
 
@@ -91,7 +96,10 @@ enum mpsb_status_bits {
     MPSB_ST_NOCONV = 1,    /* Jacobi hit max_sweeps; result written anyway */
     MPSB_ST_NONFINITE = 2, /* theta held NaN or Inf                         */
     MPSB_ST_BADDIM = 4,    /* bond dimensions out of range; pair skipped    */
-    MPSB_ST_TIMEOUT = 8    /* a bounded intra-CTA wait gave up; result invalid */
+    MPSB_ST_TIMEOUT = 8,   /* a bounded wait gave up; result invalid             */
+    MPSB_ST_CHI_LIMIT = 16 /* the keep rule asked for more than MPSB_CHI_LIMIT values
+                              (chi_max above the limit): MPSB_CHI_LIMIT were kept, so
+                              the state differs from mps_core's from here on        */
 };
 
 enum mpsb_error {
@@ -139,7 +147,9 @@ MPSB_API int mpsb_update2q_batch(const mpsb_chain *chains, const mpsb_pair *pair
  * chi_cap) that every GPU loading the library holds until exit.  Batches that
  * need more scratch are rejected with MPSB_EWORKSPACE before any launch.  The
  * first call on a device looks up the array's device address (set-up), so
- * make that first call before any stream capture.  All calls share the
+ * make that first call before any stream capture; the address is kept for the
+ * life of the process, so do not use this entry across a cudaDeviceReset
+ * of that device.  All calls share the
  * array: calls whose kernels overlap on the GPU race, serialise them on one
  * stream.  It allocates nothing (no cudaMalloc, no cudaFree). */
 #define MPSB_NOALLOC_SCRATCH_BYTES (16u << 20)

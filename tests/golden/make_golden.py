@@ -1,9 +1,9 @@
 """Generate the golden fixtures in this folder by running the reference engine.
 
-Run from the repository root in a container where the reference checkout is
-mounted (read-only) at /root/reference:
+Run from the repository root with a checkout of the reference repository,
+given as the first argument or in the environment variable MPS_REFERENCE_DIR:
 
-    python tests/golden/make_golden.py [/path/to/reference] [run_NAME ...]
+    python tests/golden/make_golden.py /path/to/reference [run_NAME ...]
 
 It imports the reference's ``mps_core.py`` unchanged, drives it through its own
 public methods (``apply_1q``, ``apply_2q``, ``_apply_adjacent_2q``,
@@ -27,7 +27,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _ARGS = [a for a in sys.argv[1:] if not a.startswith("--")]
-REF = _ARGS[0] if _ARGS and not _ARGS[0].startswith("run_") and os.path.isdir(_ARGS[0]) else "/root/reference"
+REF = _ARGS[0] if _ARGS and not _ARGS[0].startswith("run_") else os.environ.get("MPS_REFERENCE_DIR", "")
+if not REF or not os.path.isfile(os.path.join(REF, "mps_core.py")):
+    sys.exit("make_golden.py: give the reference checkout (the folder holding mps_core.py) as the first "
+             "argument or in MPS_REFERENCE_DIR")
 sys.path.insert(0, REF)
 import mps_core  # noqa: E402  (the reference module, unchanged)
 
@@ -245,6 +248,45 @@ def run_measure():
     print("measure: shots", len(shots), "distinct", len(set(shots)))
 
 
+def run_dropin():
+    """What a drop-in user of the reference class sees: entanglement_entropy and
+    bond_spectrum (mps_core.py:465-494) on every bond of two circuit states, and
+    the default bond cap (MPSState(n) keeps chi_max=256, mps_core.py:185): a
+    12-qubit circuit whose bonds stay within 64, and a 14-qubit one whose
+    middle bond needs 128."""
+    out = {}
+    for key, (n, depth, chi, cutoff, seed) in {"b16": (16, 10, 16, 1e-12, 1234),
+                                                "b20": (20, 12, 64, 1e-10, 4242)}.items():
+        st = mps_core.MPSState(n, chi, cutoff)
+        for i, g in brick(n, depth, seed):
+            st._apply_adjacent_2q(i, g)
+        spec = [st.bond_spectrum(b) for b in range(n)]
+        lens = np.array([len(x) for x in spec], np.int32)
+        sp = np.zeros((n, lens.max()))
+        for k, x in enumerate(spec):
+            sp[k, :len(x)] = x
+        out[key + "_entropy"] = np.array([st.entanglement_entropy(b) for b in range(n - 1)])
+        out[key + "_bond_spectrum"] = sp
+        out[key + "_bond_spectrum_len"] = lens
+        out[key + "_bonds"] = np.array(st.bond_dims(), np.int32)
+    for key, (n, depth, seed) in {"d12": (12, 10, 99), "d14": (14, 12, 98)}.items():
+        st = mps_core.MPSState(n)
+        gates = brick(n, depth, seed)
+        for i, g in gates:
+            st._apply_adjacent_2q(i, g)
+        bits = np.random.default_rng(seed + 1).integers(0, 2, size=(32, n))
+        out[key + "_chi_max"] = st.chi_max
+        out[key + "_cutoff"] = st.svd_cutoff
+        out[key + "_sites"] = np.array([i for i, _ in gates], np.int32)
+        out[key + "_gates"] = np.stack([g for _, g in gates])
+        out[key + "_bonds"] = np.array(st.bond_dims(), np.int32)
+        out[key + "_norm_log"] = st.norm_log
+        out[key + "_bits"] = bits.astype(np.int8)
+        out[key + "_amps"] = amplitudes(st, bits)
+    np.savez_compressed(os.path.join(HERE, "dropin.npz"), **out)
+    print("dropin: max bonds", out["d12_bonds"].max(), out["d14_bonds"].max())
+
+
 class _Q:
     def __init__(self, i):
         self.index = i
@@ -357,6 +399,7 @@ RUNS = {
     "run_xxz": run_xxz,
     "run_measure": run_measure,
     "run_compiler": run_compiler,
+    "run_dropin": run_dropin,
 }
 
 if __name__ == "__main__":

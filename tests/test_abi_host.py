@@ -64,6 +64,16 @@ def test_argument_errors_need_no_device():
         _lib.check(-1, "probe")
 
 
+def test_keep_limit_and_status_names():
+    # min(chi_max, the device limit 64, the Schmidt bound 2^(n//2) of an n-site chain)
+    assert _lib.keep_limit(12, 256) == 64 and _lib.keep_limit(8, 256) == 16
+    assert _lib.keep_limit(100, 32) == 32 and _lib.keep_limit(1, 256) == 1 and _lib.keep_limit(5, 3) == 3
+    assert _lib.status_text(0) == "ok"
+    assert "bond above 64" in _lib.status_text(_lib.ST_CHI_LIMIT | _lib.ST_NOCONV)
+    hdr = open(HEADER).read()
+    assert re.search(r"MPSB_ST_CHI_LIMIT\s*=\s*16", hdr) and re.search(r"MPSB_ST_TIMEOUT\s*=\s*8", hdr)
+
+
 def test_validate_pairs():
     validate_pairs([10], [0, 0, 0], [0, 2, 8])
     validate_pairs([10, 6], [0, 0, 1, 1], [1, 5, 0, 4])

@@ -141,4 +141,4 @@ def test_schmidt_values_and_entropy_match_dense_state():
         assert len(got) >= np.count_nonzero(s > 1e-12)
         np.testing.assert_allclose(got[:len(s)][s > 1e-12], s[s > 1e-12], atol=1e-12)
         p = s ** 2
-        assert abs(st.entanglement_entropy(bond) + float(np.sum(p * np.log(p)))) < 1e-10
+        assert abs(st.exact_entanglement_entropy(bond) + float(np.sum(p * np.log(p)))) < 1e-10

@@ -4,6 +4,7 @@ contiguous and disjoint, and orders / groups chains as the strategy says."""
 import numpy as np
 import pytest
 
+from fpga_mps_simulator_b200._lib import keep_limit
 from fpga_mps_simulator_b200.circuits import random_circuit_batch
 from fpga_mps_simulator_b200.mps import validate_pairs
 from fpga_mps_simulator_b200.schedule import STRATEGIES, Schedule
@@ -22,6 +23,7 @@ class _FakeBatch:
     def __init__(self, specs):
         self.ns = [s.n for s in specs]
         self.chi_maxs = [s.chi_max for s in specs]
+        self.caps = [keep_limit(s.n, s.chi_max) for s in specs]
 
     @property
     def nchains(self):
@@ -46,7 +48,7 @@ def test_strategy_covers_every_pair_once(specs, strategy):
     for L, launches in enumerate(plan):
         seen = {}
         for lc in launches:
-            assert lc.chi_cap >= max(b.chi_maxs[c] for c in lc.pb.ci)
+            assert lc.chi_cap >= max(b.caps[c] for c in lc.pb.ci)
             for c, i, g in zip(lc.pb.ci, lc.pb.si, lc.pb.gates):
                 assert (c, i) not in seen
                 seen[(c, i)] = g
@@ -64,13 +66,13 @@ def test_lpt_orders_by_decreasing_cost_and_split_groups_by_cap(specs):
     sch = Schedule(b, [s.layers for s in specs])
     for launches in sch.launches("lpt"):
         assert len(launches) == 1
-        caps = [b.chi_maxs[c] for c in launches[0].pb.ci]
+        caps = [b.caps[c] for c in launches[0].pb.ci]
         assert caps == sorted(caps, reverse=True)
     for launches in sch.launches("split"):
         caps = [lc.chi_cap for lc in launches]
         assert caps == sorted(set(caps), reverse=True)
         for lc in launches:
-            assert {b.chi_maxs[c] for c in lc.pb.ci} == {lc.chi_cap}
+            assert {b.caps[c] for c in lc.pb.ci} == {lc.chi_cap}
 
 
 def test_unknown_strategy_rejected(specs):

@@ -6,7 +6,9 @@ cudaMalloc would synchronise the device): it keeps its scratch in a fixed
 16 MiB device array instead of a caller workspace.  This test drives both
 entry points through the C ABI on identical chains, two calls in a row, and
 requires the same spectra, kept counts, bonds, norm_log and amplitudes within
-the FP64 parity tolerance; it also checks that an oversized batch is refused
+the FP64 parity tolerance, in both forms (at chi_cap = 64 the mixed form is the
+tensor-core kernel with its own shared-memory size and cutoff floor); it also
+checks that an oversized batch is refused
 before anything is launched.  It lives in the last test file so that a run
 stopping at the first failure has already run every other test.
 """
@@ -18,14 +20,16 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-10
 
 
-def test_noalloc_matches_workspace_entry_two_calls():
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_noalloc_matches_workspace_entry_two_calls(precision):
     from fpga_mps_simulator_b200 import MPSBatch, _lib
     from fpga_mps_simulator_b200.circuits import brickwall_layers
 
     lib = _lib.load()
     n, chi, cut = 24, 64, 1e-10
-    ref = MPSBatch([n], [chi], [cut])
-    new = MPSBatch([n], [chi], [cut])
+    code = _lib.FP64 if precision == "fp64" else _lib.MIXED_TF32X3
+    ref = MPSBatch([n], [chi], [cut], precision=precision)
+    new = MPSBatch([n], [chi], [cut], precision=precision)
     layers = brickwall_layers(n, 8, 321)
     # bring both chains to a saturated state the same way
     for L in layers[:6]:
@@ -37,7 +41,7 @@ def test_noalloc_matches_workspace_entry_two_calls():
         ref.run_pairs(pa)
         pb = new.make_pairs(np.zeros(len(L.sites), np.int32), L.sites, L.gates, record_spectra=True)
         rc = lib.mpsb_update2q_batch_noalloc(new.table.data_ptr(), pb.pairs.data_ptr(), pb.npairs,
-                                             pb.gates.data_ptr(), _lib.FP64, new.chi_cap, 0.0, 0,
+                                             pb.gates.data_ptr(), code, new.chi_cap, 0.0, 0,
                                              pb.spectra.data_ptr(), pb.kept.data_ptr(), pb.trunc.data_ptr(),
                                              pb.status.data_ptr(), stream)
         _lib.check(rc, "mpsb_update2q_batch_noalloc")
