@@ -3,14 +3,16 @@
 
 Workload (one "step"): a 100-qubit open chain in |0...0>, depth-20 brick-wall
 of Haar-random 4x4 gates (seeded), chi_max = 64, cutoff 1e-10 -- 990 two-site
-updates, each layer's 49-50 disjoint pairs in one launch.  Synthetic gates;
-no dataset is involved.
+updates, all 20 layers in one dataflow launch (each pair starts when the two
+updates before it on its sites are done); one launch per layer (49-50 pairs
+each) is timed beside it, with bit-identical results.  Synthetic gates; no
+dataset is involved.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 ``value`` is device-timed (CUDA events, inputs resident in HBM, L2 flushed
 between steps) updates/s over all ranks; ``e2e`` runs the same circuit
-through the public Python API (``MPSState.apply_layer``) with the gates copied
+through the public Python API (``MPSState.apply_layers``) with the gates copied
 from pinned host memory and the final MPS read back every step.  With
 --gpus N > 1 (launched by torch.distributed.run) every rank advances its own
 replica circuit (different seed): no collective on the data path, timing is
@@ -38,14 +40,15 @@ METRIC = "MPS 2-site updates/s at chi=64 and grad s/step: mixed vs FP64 GPU, err
 UNIT = "updates/s"
 N_SITES, DEPTH, CHI, CUTOFF, SEED = 100, 20, 64, 1e-10, 2024
 WORKLOAD = (f"MPS two-site updates: n={N_SITES} open chain, depth-{DEPTH} Haar brick-wall, "
-            f"chi_max={CHI}, cutoff={CUTOFF:g}, each layer's pairs in one launch")
+            f"chi_max={CHI}, cutoff={CUTOFF:g}; all layers' pairs in one dataflow launch "
+            "(per-layer launches reported beside it)")
 
 
-# DRAM bytes (read + write) of one saturated-layer launch of the update kernel
-# (49 pairs at chi = 64, mixed form), from one ncu capture of this workload.
-TRAFFIC_PER_LAUNCH = 11.99e6
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one saturated-layer launch "
-                  "(layer 19 of this workload); algorithmic site reads 12.8 MB")
+# DRAM bytes (read + write) of one dataflow launch (the whole 990-update step,
+# mixed form), from one ncu capture of this workload; None until measured.
+TRAFFIC_PER_LAUNCH = None
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one dataflow launch of this "
+                  "workload (990 updates); algorithmic site bytes per step in hbm_site_bytes_per_step")
 
 # ----------------------------------------------------------------- counting
 def update_flops(cl: int, cm: int, cr: int) -> float:
@@ -87,7 +90,7 @@ def batching_leg(dev, steps: int, rank: int, max_over_ranks, precision: str = "m
     import torch
     from fpga_mps_simulator_b200 import MPSBatch
     from fpga_mps_simulator_b200.circuits import random_circuit_batch
-    from fpga_mps_simulator_b200.schedule import Runner, Schedule, autotune, last_timings
+    from fpga_mps_simulator_b200.schedule import Runner, Schedule, autotune, last_shapes, last_timings
 
     specs = random_circuit_batch(BATCH_CIRCUITS, seed=SEED + rank, n_range=BATCH_N, depth_range=BATCH_DEPTH,
                                  chis=BATCH_CHIS)
@@ -97,6 +100,8 @@ def batching_leg(dev, steps: int, rank: int, max_over_ranks, precision: str = "m
     init = b.snapshot()
     best = autotune(sch, start=12, layers=4, repeats=2)
     tuned = dict(last_timings)
+    shapes = {k: dict(v) for k, v in last_shapes.items()}
+    flow_threads = {f"chi{k}": v for k, v in sch.flow_threads.items()}
     r = Runner(sch, best)
     r.capture()
 
@@ -137,10 +142,13 @@ def batching_leg(dev, steps: int, rank: int, max_over_ranks, precision: str = "m
                          f"{precision} form"),
             "updates_per_run": n_upd, "strategy": best, "launches_per_run": launches,
             "autotune_ms": {k: round(v, 3) for k, v in tuned.items()},
+            "flow_cta_threads": flow_threads, "flow_shape_ms": shapes,
             "graph_updates_per_s": round(n_upd / graph_s, 3), "graph_s_per_run": round(graph_s, 4),
             "loop_updates_per_s": round(n_upd / loop_s, 3), "loop_s_per_run": round(loop_s, 4),
             "speedup_vs_loop": round(loop_s / graph_s, 3),
-            "note": "graph = whole run captured as one CUDA graph; loop = one launch per circuit layer"}
+            "note": ("graph = whole run captured as one CUDA graph; loop = one launch per circuit layer; "
+                     "strategies: single / lpt / split launch per layer, flow = one dataflow launch per "
+                     "bond-cap class for all layers (CTA threads per class picked by the autotuner)")}
 
 
 GRAD_N, GRAD_LAYERS, GRAD_VEC, GRAD_CHI, GRAD_CUT = 64, 8, 64, 32, 1e-12
@@ -300,10 +308,10 @@ def gradient_leg(dev, steps: int, warmup: int, rank: int, max_over_ranks, cpu_wo
         "config": check, f"control_{ctl_layers}_layers": control,
         "bar": "adjoint within 1e-5 of parameter shift, relative to the largest |gradient|",
         "note": ("parameter shift and central differences run the plain FP64 forward on one parameter vector; "
-                 "at 8 layers the bonds saturate at chi_max=32 and truncation makes the forward only piecewise "
-                 "smooth, so neither parameter shift (exact only for an untruncated circuit) nor a finite "
-                 "difference across a truncation boundary is the derivative the adjoint computes; the "
-                 f"{ctl_layers}-layer control (no chi truncation) is where the 1e-5 bar applies")}
+                 "at 8 layers the bonds saturate at chi_max=32: the truncated energy is no longer a sinusoid "
+                 "in each angle, so the parameter-shift rule itself stops being a derivative (compare "
+                 "parameter_shift_vs_fd), while central differences still measure the derivative the adjoint "
+                 f"computes; the {ctl_layers}-layer control has no chi truncation, where all three agree")}
     if cpu_workers:
         from oracle.cpu_baseline import make_pool, run_forward_parallel, run_grad_parallel
         pool = make_pool(cpu_workers)
@@ -610,12 +618,62 @@ def run_ours(args) -> None:
                 "flops": flops, "hbm": hbm, "kern_s": kern_s, "clocks": clk,
                 "achieved_tf": flops / kern_s / 1e12, "trunc": trunc}
 
-    main = measure(precision, timed=True)
+    # per-layer launches (one launch per layer), both forms: the reference point and the state checks
+    main = measure(precision, timed=False)
     other_prec = "fp64" if precision == "mixed" else "mixed"
     other = measure(other_prec, timed=False)
-    value, total_s = main["value"], main["total_s"]
-    mixed_v, fp64_v = (value, other["value"]) if precision == "mixed" else (other["value"], value)
-    flops, hbm, kern_s, achieved_tf, clk = main["flops"], main["hbm"], main["kern_s"], main["achieved_tf"], main["clocks"]
+
+    def measure_flow(prec: str, timed: bool, ref: dict):
+        """The same circuit as ONE dataflow launch (all 20 layers; each pair starts when its two
+        predecessors are done), device-timed like the per-layer steps: reset + launch per step,
+        L2 flushed before each; the launch alone is timed for the roofline."""
+        batch = MPSBatch([N_SITES], [CHI], [CUTOFF], precision=prec, device=dev,
+                         tol=args.mixed_tol if prec == "mixed" else 0.0)
+        fb = batch.make_flow(np.concatenate([np.zeros(len(L.sites), np.int32) for L in layers]),
+                             np.concatenate([L.sites for L in layers]), np.concatenate([L.gates for L in layers]))
+        for _ in range(args.warmup):
+            reset(batch)
+            batch.run_flow(fb)
+        torch.cuda.synchronize()
+        batch.check_status()
+        clocks = ClockSampler(gpu_id) if timed else None
+        barrier()
+        torch.cuda.synchronize()
+        step_ms, kern_ms = [], []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            e0.record()
+            reset(batch)
+            e1.record()
+            batch.run_flow(fb)
+            e2.record()
+            torch.cuda.synchronize()
+            step_ms.append(e0.elapsed_time(e2))
+            kern_ms.append(e1.elapsed_time(e2))
+        torch.cuda.synchronize()
+        barrier()
+        clk = clocks.stop() if clocks else None
+        batch.check_status()
+        total_s = max_over_ranks(sum(step_ms) * 1e-3)
+        kern_s = sum(kern_ms) * 1e-3 / args.steps
+        same = all(torch.equal(x, y) for x, y in zip(batch.snapshot(), ref["batch"].snapshot()))
+        return {"value": world * n_upd * args.steps / total_s, "total_s": total_s, "kern_s": kern_s,
+                "clocks": clk, "achieved_tf": ref["flops"] / kern_s / 1e12, "bitwise_equal_to_per_layer": same}
+
+    fmain = measure_flow(precision, True, main)
+    fother = measure_flow(other_prec, False, other)
+    value, total_s = fmain["value"], fmain["total_s"]
+    mixed_v, fp64_v = (value, fother["value"]) if precision == "mixed" else (fother["value"], value)
+    flops, hbm, kern_s, achieved_tf, clk = main["flops"], main["hbm"], fmain["kern_s"], fmain["achieved_tf"], fmain["clocks"]
+    flow = {"per_layer_launches": {precision: round(main["value"], 3), other_prec: round(other["value"], 3)},
+            "one_dataflow_launch": {precision: round(value, 3), other_prec: round(fother["value"], 3)},
+            f"{precision}_bitwise_equal": fmain["bitwise_equal_to_per_layer"],
+            f"{other_prec}_bitwise_equal": fother["bitwise_equal_to_per_layer"],
+            "note": ("value = one dataflow launch per step (all 20 layers: a cluster per update, claimed in "
+                     "layer order, started when its two predecessors finish, + one norm_log fold); "
+                     "per_layer_launches = 20 launches per step, each layer's pairs in one; final states "
+                     "compared bit for bit")}
     from fpga_mps_simulator_b200.mps import overlap
     ab, lab = overlap(main["batch"], 0, other["batch"], 0)
     aa, laa = overlap(main["batch"], 0, main["batch"], 0)
@@ -676,13 +734,14 @@ def run_ours(args) -> None:
     e2e = None
     if not args.quick:
         st = MPSState(N_SITES, CHI, CUTOFF, precision=precision, device=dev)
-        pinned = [torch.from_numpy(np.ascontiguousarray(L.gates)).pin_memory() for L in layers]
+        pinned = torch.from_numpy(np.ascontiguousarray(np.concatenate([L.gates for L in layers]))).pin_memory()
         ones = torch.ones(N_SITES, dtype=torch.complex128).pin_memory()
         out_sites = torch.empty(st._b.sites.shape, dtype=torch.complex128).pin_memory()
         out_bonds = torch.empty(N_SITES + 1, dtype=torch.int32).pin_memory()
         out_nl = torch.empty(1, dtype=torch.float64).pin_memory()
-        h2d = sum(p.numel() * 16 for p in pinned) + sum(len(L.sites) * 16 for L in layers) + N_SITES * 16
+        h2d = pinned.numel() * 16 + N_SITES * 16
         d2h = out_sites.numel() * 16 + out_bonds.numel() * 4 + 8
+        flow_tables = [None]  # built by the first (untimed) call, then reused: only the gates travel
 
         def e2e_step():
             b = st._b
@@ -690,8 +749,7 @@ def run_ours(args) -> None:
             b.sites[:, 0].copy_(ones, non_blocking=True)
             b.bonds.fill_(1)
             b.norm_logs.zero_()
-            for L, g in zip(layers, pinned):
-                st.apply_layer(L.sites, g)
+            flow_tables[0] = st.apply_layers([L.sites for L in layers], pinned, flow=flow_tables[0])
             out_sites.copy_(b.sites, non_blocking=True)
             out_bonds.copy_(b.bonds, non_blocking=True)
             out_nl.copy_(b.norm_logs, non_blocking=True)
@@ -716,6 +774,7 @@ def run_ours(args) -> None:
     if not args.quick and not args.no_gradient:
         from oracle.cpu_baseline import usable_cores
         cw = usable_cores() if (rank == 0 and world == 1 and not args.no_cpu) else 0
+        torch.cuda.empty_cache()  # the 7.6 GB of tapes below should not fight the earlier legs' cached blocks
         gradient = gradient_leg(dev, 5, 3, rank, max_over_ranks, cpu_workers=cw)
         for key in ("fp64", "mixed", "fp64_checkpointed"):  # fraction of the same FP64 roofline
             gradient[key]["roofline_frac"] = round(gradient[key]["achieved_tflops"] / fp64_peak_tflops, 4)
@@ -727,9 +786,10 @@ def run_ours(args) -> None:
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_s * 1e3 / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f64+tf32x3",
-        "forms": {precision: round(value, 3), other_prec: round(other["value"], 3),
+        "forms": {precision: round(value, 3), other_prec: round(fother["value"], 3),
                   "infidelity_mixed_vs_fp64": infid, **form_errors,
                   "infidelity_mixed_vs_fp64_by_depth": by_depth,
+                  "launch_modes": flow,
                   "note": "batched per layer; mixed = 3xTF32 tcgen05 complex-3M theta + FP64 Jacobi SVD"},
         "target_ratio": {
             "batched_mixed_over_batched_fp64": round(mixed_v / fp64_v, 3),
@@ -741,16 +801,16 @@ def run_ours(args) -> None:
                      "second reading: the plain form as the drop-in calls it, one update per launch")},
         "data": "synthetic (seeded Haar-random 4x4 gates, |0...0> start)",
         "config": {"workload": WORKLOAD, "precision": precision, "updates_per_step": n_upd,
-                   "launches_per_step": 2 * len(layers), "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "launches_per_step": 2, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "flushed between steps (256 MiB write)"},
         "roofline": {"bound": "fp64", "achieved": round(achieved_tf, 4), "peak": round(fp64_peak_tflops, 4),
                      "unit": "TFLOP/s", "frac": round(achieved_tf / fp64_peak_tflops, 4),
                      "traffic": TRAFFIC_PER_LAUNCH, "traffic_source": TRAFFIC_SOURCE,
                      "peak_source": "measured: FP64 FMA probe (mpsb_fp64_probe) on this GPU, burst",
-                     "kernel": f"update2q kernel ({precision}) + fold_norm_log_kernel",
+                     "kernel": f"update2q_flow_kernel ({precision}) + fold_flow_kernel",
                      "flops_per_step": flops, "hbm_site_bytes_per_step": hbm,
                      "hbm_gbs": round(hbm / kern_s / 1e9, 3)},
-        "gpu_launches": 2 * len(layers) * args.steps,
+        "gpu_launches": 2 * args.steps,
         "clocks": clk,
         "e2e": e2e,
         "per_update_path": single,
@@ -795,7 +855,10 @@ def main():
                     help="run one secondary leg alone and print its JSON (profiling)")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the 1000-qubit XXZ initial-state gradient leg (about a minute)")
+    ap.add_argument("--grad-vectors", type=int, default=64,
+                    help="parameter vectors of the gradient leg (fewer: a small case for profiling)")
     args = ap.parse_args()
+    globals()["GRAD_VEC"] = args.grad_vectors
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":

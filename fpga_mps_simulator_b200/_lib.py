@@ -35,7 +35,16 @@ EXPORTS = (
     "mpsb_update2q_backward_batch", "mpsb_apply1q_backward_batch", "mpsb_mpo_grad_workspace_bytes",
     "mpsb_mpo_energy_grad", "mpsb_sample_workspace_bytes", "mpsb_sample", "mpsb_reset_batch",
     "mpsb_canonicalize_workspace_bytes", "mpsb_canonicalize",
+    "mpsb_update2q_flow_workspace_bytes", "mpsb_update2q_flow_clusters", "mpsb_update2q_flow",
 )
+
+# CTA sizes (threads) the dataflow kernel is built for, by rows per lane
+# (1: chi_cap <= 16, 2: <= 32, 4: <= 64); the first is the default.
+FLOW_THREADS = {1: (64, 128), 2: (128, 256), 4: (256,)}
+
+
+def rows_per_lane(chi_cap: int) -> int:
+    return 1 if 2 * chi_cap <= 32 else (2 if 2 * chi_cap <= 64 else 4)
 
 
 class Chain(C.Structure):
@@ -55,6 +64,12 @@ class Chain(C.Structure):
 class Pair(C.Structure):
     """mpsb_pair."""
     _fields_ = [("chain", C.c_int32), ("site", C.c_int32), ("gate", C.c_int32), ("out", C.c_int32)]
+
+
+class FlowItem(C.Structure):
+    """mpsb_flow_item."""
+    _fields_ = [("chain", C.c_int32), ("site", C.c_int32), ("gate", C.c_int32), ("out", C.c_int32),
+                ("dep0", C.c_int32), ("dep1", C.c_int32)]
 
 
 class SiteOp(C.Structure):
@@ -97,6 +112,10 @@ def _declare(lib):
         "mpsb_reset_batch": (i32, [vp, vp, i32, i32, vp]),
         "mpsb_canonicalize_workspace_bytes": (sz, [i32, i32]),
         "mpsb_canonicalize": (i32, [vp, vp, i32, i32, i32, i32, i32, vp, sz, vp]),
+        "mpsb_update2q_flow_workspace_bytes": (sz, [i32, i32, i32, i32, i32]),
+        "mpsb_update2q_flow_clusters": (i32, [i32, i32, i32]),
+        "mpsb_update2q_flow": (i32, [vp, i32, vp, i32, vp, vp, vp, i32, i32, dbl, i32, i32, i32, i32, vp, sz,
+                                     vp, vp, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

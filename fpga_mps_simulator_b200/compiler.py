@@ -370,7 +370,8 @@ class MPSSimulator:
         for idx, (n, prog, meas) in enumerate(compiled):
             st = MPSState(n, self.chi_max, self.svd_cutoff, self.precision, batch.device)
             o = int(batch.site_off[idx])
-            st._b.sites[:n].copy_(batch.sites[o:o + n])
+            # the chain's bonds fit its own cap, so the head of each batch slot holds the whole site
+            st._b.sites[:n].copy_(batch.sites[o:o + n, : st._b.slot])
             b0 = int(batch.bond_off[idx])
             st._b.bonds.copy_(batch.bonds[b0:b0 + n + 1])
             st._b.norm_logs[0] = batch.norm_logs[idx]

@@ -54,7 +54,22 @@ struct BwdParams {
     int chi_cap;
     double retain;
     double broaden;
+    int pqg_in_smem;         // P, Q and G' in dynamic shared memory (chi_cap <= 32) instead of the scratch
 };
+
+// The per-pair scratch is dead once a pair is done: drop its lines from L2
+// without writing them back (the next pair writes every element before it
+// reads it).  Without this, the tapes streaming through L2 evicted the dirty
+// scratch to DRAM -- most of the backward's DRAM writes.
+__device__ __forceinline__ void discard_l2(const double2 *base, size_t n_elems, int tid, int nthreads) {
+    const char *b = reinterpret_cast<const char *>(base);
+    const size_t lines = n_elems * sizeof(double2) / 128;
+    for (size_t l = tid; l < lines; l += nthreads)
+        asm volatile("discard.global.L2 [%0], 128;" ::"l"(b + l * 128) : "memory");
+}
+
+// Tape elements are read once per backward: streaming loads (evict first).
+__device__ __forceinline__ double2 ld_tape(const double2 *p) { return __ldcs(p); }
 
 // One pair; every early exit is block-uniform.  `base` is this CTA's scratch.
 __device__ __forceinline__ void backward_pair(const BwdParams &p, const int pi, double2 *base) {
@@ -118,13 +133,15 @@ __device__ __forceinline__ void backward_pair(const BwdParams &p, const int pi, 
     const double2 *Asite = reinterpret_cast<const double2 *>(ch.sites + (size_t)site * ch.slot_elems);
     const double2 *Bsite = reinterpret_cast<const double2 *>(ch.sites + (size_t)(site + 1) * ch.slot_elems);
 
+    extern __shared__ __align__(16) double2 bwd_dyn[];
     double2 *U = base;                       // R x rp
     double2 *V = base + Qn;                  // C x rp
     double2 *Ub = base + 2 * Qn;             // R x K
     double2 *Vb = base + 2 * Qn + Qn / 2;    // C x K
-    double2 *Pm = base + 3 * Qn;             // rp x K
-    double2 *Qm = base + 3 * Qn + Qn / 2;    // rp x K
-    double2 *Gm = base + 4 * Qn;             // rp x rp
+    double2 *const pqg = p.pqg_in_smem ? bwd_dyn : base + 3 * Qn;
+    double2 *Pm = pqg;                       // rp x K
+    double2 *Qm = pqg + Qn / 2;              // rp x K
+    double2 *Gm = pqg + Qn;                  // rp x rp
     double2 *T = base + 5 * Qn;              // R x rp
     double2 *Mb = base + 6 * Qn;             // 2cl x 2cr
     double2 *Th = base + 7 * Qn;             // 2cl x 2cr (gate cotangent only)
@@ -147,24 +164,24 @@ __device__ __forceinline__ void backward_pair(const BwdParams &p, const int pi, 
         // 2'. V = Vs / S (the QR-preconditioned forward taped the right side)
         for (int e = tid; e < C * rp; e += kBwdThreads) {
             const int i = e / rp, j = e - i * rp;
-            V[e] = c_scale(Xs[(size_t)j * C + i], 1.0 / sS[j]);
+            V[e] = c_scale(ld_tape(Xs + (size_t)j * C + i), 1.0 / sS[j]);
         }
         __syncthreads();
         // 3'. U = X V S^-1   (R x rp)
         cta_cgemm<true, true>(
-            R, rp, C, [&](int r, int k) { return X[(size_t)r * C + k]; },
+            R, rp, C, [&](int r, int k) { return ld_tape(X + (size_t)r * C + k); },
             [&](int k, int j) { return V[(size_t)k * rp + j]; },
             [&](int r, int j, double2 v) { U[(size_t)r * rp + j] = c_scale(v, 1.0 / sS[j]); }, sm);
     } else {
         // 2. U = Xs / S
         for (int e = tid; e < R * rp; e += kBwdThreads) {
             const int r = e / rp, j = e - r * rp;
-            U[e] = c_scale(Xs[(size_t)j * R + r], 1.0 / sS[j]);
+            U[e] = c_scale(ld_tape(Xs + (size_t)j * R + r), 1.0 / sS[j]);
         }
         __syncthreads();
         // 3. V = X^H U S^-1   (C x rp)
         cta_cgemm<false, true>(
-            C, rp, R, [&](int i, int k) { return c_conj(X[(size_t)k * C + i]); },
+            C, rp, R, [&](int i, int k) { return c_conj(ld_tape(X + (size_t)k * C + i)); },
             [&](int k, int j) { return U[(size_t)k * rp + j]; },
             [&](int i, int j, double2 v) { V[(size_t)i * rp + j] = c_scale(v, 1.0 / sS[j]); }, sm);
     }
@@ -304,6 +321,8 @@ __device__ __forceinline__ void backward_pair(const BwdParams &p, const int pi, 
             [&](int k, int j) { return Mb[(size_t)k * twocr + j]; },
             [&](int i, int j, double2 v) { Bcot[(size_t)i * twocr + j] = v; }, sm);
     }
+    __syncthreads();
+    discard_l2(base, (size_t)8 * Qn, tid, kBwdThreads);
     if (tid == 0) p.status[pr.out] = 0;
 }
 
@@ -640,7 +659,13 @@ int launch_update2q_backward(const mpsb_chain *pre, const mpsb_chain *cot, const
     p.chi_cap = chi_cap;
     p.retain = retain;
     p.broaden = broaden;
-    update2q_backward_kernel<<<std::min(npairs, bwd_grid_cap()), kBwdThreads, 0, s>>>(p);
+    // P, Q (rp x K each, <= Q/2) and G' (rp x rp, <= Q) fit in shared memory up to chi_cap = 32
+    p.pqg_in_smem = chi_cap <= 32 ? 1 : 0;
+    const size_t dyn = p.pqg_in_smem ? (size_t)2 * (2 * chi_cap) * (2 * chi_cap) * sizeof(double2) : 0;
+    const int rc = ensure_smem(reinterpret_cast<const void *>(update2q_backward_kernel), dyn,
+                               "cudaFuncSetAttribute(update2q_backward)");
+    if (rc) return rc;
+    update2q_backward_kernel<<<std::min(npairs, bwd_grid_cap()), kBwdThreads, dyn, s>>>(p);
     return check_launch("update2q_backward_kernel");
 }
 

@@ -89,6 +89,11 @@ int launch_expect(const mpsb_chain *, int, int, int, const int32_t *, const int3
 int launch_fp64_probe(long long iters, int blocks, int threads, double *sink, cudaStream_t s);
 int launch_overlap(const mpsb_chain *, const mpsb_chain *, int, int, double2 *, double *, void *, cudaStream_t);
 
+size_t upd_flow_workspace_bytes(int nitems, int chi_cap, int precision, int threads, int nclusters);
+int upd_flow_clusters(int chi_cap, int precision, int threads);
+int launch_update2q_flow(const mpsb_chain *, int, const mpsb_flow_item *, int, const int32_t *, const int32_t *,
+                         const double2 *, int, int, double, int, int, int, int, void *, size_t, double *, int32_t *,
+                         double *, int32_t *, cudaStream_t);
 size_t upd_tape_bytes(int npairs, int chi_cap);
 int launch_update2q_taped(bool, const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int,
                           void *, void *, double *, int32_t *, double *, int32_t *, cudaStream_t);
@@ -159,6 +164,47 @@ int mpsb_update2q_batch(const mpsb_chain *chains, const mpsb_pair *pairs, int np
     if (tol <= 0.0) tol = 1.0e-9;
     return launch_update2q_mixed(chains, pairs, npairs, g, chi_cap, tol, max_sweeps, workspace, spectra, kept,
                                  trunc, status, s);
+}
+
+size_t mpsb_update2q_flow_workspace_bytes(int nitems, int chi_cap, int precision, int threads, int nclusters) {
+    if (nitems < 0 || chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT) return 0;
+    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3) return 0;
+    return upd_flow_workspace_bytes(nitems, chi_cap, precision, threads, nclusters);
+}
+
+int mpsb_update2q_flow_clusters(int chi_cap, int precision, int threads) {
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3)
+        return set_error(MPSB_EINVAL, "unknown precision %d", precision);
+    int rc = check_device(nullptr, nullptr);
+    if (rc) return rc;
+    return upd_flow_clusters(chi_cap, precision, threads);
+}
+
+int mpsb_update2q_flow(const mpsb_chain *chains, int nchains, const mpsb_flow_item *items, int nitems,
+                       const int32_t *chain_order, const int32_t *chain_offsets, const mpsb_c128 *gates,
+                       int precision, int chi_cap, double tol, int max_sweeps, int threads, int nclusters,
+                       int poll_limit, void *workspace, size_t workspace_bytes, double *spectra, int32_t *kept,
+                       double *trunc, int32_t *status, mpsb_stream_t stream) {
+    if (nitems < 0 || nchains < 0) return set_error(MPSB_EINVAL, "nitems=%d / nchains=%d < 0", nitems, nchains);
+    if (nitems == 0) return MPSB_OK;
+    if (!chains || !items || !chain_order || !chain_offsets || !gates || !status || !workspace)
+        return set_error(MPSB_EINVAL, "null chains/items/chain_order/chain_offsets/gates/status/workspace pointer");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3)
+        return set_error(MPSB_EINVAL, "unknown precision %d", precision);
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
+        return set_error(MPSB_EINVAL, "workspace must be 256-byte aligned");
+    int rc = check_device(chains, stream);
+    if (rc) return rc;
+    if (max_sweeps <= 0) max_sweeps = 40;
+    if (tol <= 0.0) tol = precision == MPSB_FP64 ? 1.0e-14 : 1.0e-9;
+    return launch_update2q_flow(chains, nchains, items, nitems, chain_order, chain_offsets,
+                                reinterpret_cast<const double2 *>(gates), precision, chi_cap, tol, max_sweeps,
+                                threads, nclusters, poll_limit, workspace, workspace_bytes, spectra, kept, trunc,
+                                status, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int mpsb_apply1q_batch(const mpsb_chain *chains, const mpsb_site_op *ops, int nops, const mpsb_c128 *gates,
@@ -348,6 +394,8 @@ int mpsb_update2q_backward_batch(const mpsb_chain *pre, const mpsb_chain *cot, c
     const size_t need = bwd_workspace_bytes(npairs, chi_cap);
     if (workspace_bytes < need)
         return set_error(MPSB_EWORKSPACE, "workspace of %zu bytes < %zu needed", workspace_bytes, need);
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)  // its L2 lines are discarded per pair
+        return set_error(MPSB_EINVAL, "workspace must be 256-byte aligned");
     int rc = check_device(pre, stream);
     if (rc) return rc;
     return launch_update2q_backward(pre, cot, pairs, npairs, reinterpret_cast<const double2 *>(gates), chi_cap, tape,

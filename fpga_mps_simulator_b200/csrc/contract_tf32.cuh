@@ -135,9 +135,17 @@ __device__ __forceinline__ double part(double2 v, int prod) {
 
 // Stage the hi/lo tf32 operands of product `prod` into shared memory:
 // Ahi | Alo (128 x kpad each) then Bhi | Blo (npad x kpad each).
-template <int NT>
+// COHERENT (the persistent kernel): the sites were written by other CTAs of
+// the same launch, so they are read through L2 rather than L1.
+template <int NT, bool COHERENT = false>
 __device__ void stage_operands(unsigned char *buf, const double2 *A, const double2 *B, int cl, int cm, int cr,
                                bool trans, int idx0, const TcShape &sh, int prod, int tid) {
+    auto ld = [](const double2 *q) -> double2 {
+        if constexpr (COHERENT)
+            return __ldcg(q);
+        else
+            return *q;
+    };
     const int kc = sh.kpad >> 2;
     const uint32_t abytes = 128u * sh.kpad * 4u, bbytes = static_cast<uint32_t>(sh.npad) * sh.kpad * 4u;
     unsigned char *ahi = buf, *alo = buf + abytes, *bhi = buf + 2 * abytes, *blo = buf + 2 * abytes + bbytes;
@@ -153,9 +161,9 @@ __device__ void stage_operands(unsigned char *buf, const double2 *A, const doubl
             double v = 0.0;
             if (m < sh.mvalid && k < cm) {
                 if (!trans) {  // A[a, p, k] with m = 2a + p
-                    v = part(A[(size_t)m * cm + k], prod);
+                    v = part(ld(A + (size_t)m * cm + k), prod);
                 } else {       // B[k, q, d] with m = 2d + q
-                    v = part(B[(size_t)(2 * k + (m & 1)) * cr + (m >> 1)], prod);
+                    v = part(ld(B + (size_t)(2 * k + (m & 1)) * cr + (m >> 1)), prod);
                 }
             }
             tc::split_tf32(v, h[q], l[q]);
@@ -176,9 +184,9 @@ __device__ void stage_operands(unsigned char *buf, const double2 *A, const doubl
             double v = 0.0;
             if (n < sh.nvalid && k < cm) {
                 if (!trans) {  // B[k, q, d] with n = 2(d - idx0) + q
-                    v = part(B[(size_t)(2 * k + (n & 1)) * cr + idx0 + (n >> 1)], prod);
+                    v = part(ld(B + (size_t)(2 * k + (n & 1)) * cr + idx0 + (n >> 1)), prod);
                 } else {       // A[a, p, k] with n = 2(a - idx0) + p
-                    v = part(A[(size_t)(2 * (idx0 + (n >> 1)) + (n & 1)) * cm + k], prod);
+                    v = part(ld(A + (size_t)(2 * (idx0 + (n >> 1)) + (n & 1)) * cm + k), prod);
                 }
             }
             tc::split_tf32(v, h[q], l[q]);
@@ -279,8 +287,10 @@ __device__ void read_theta(uint32_t tmem, const TcShape &sh, const double2 *g, b
 
 // Whole mixed-precision contraction of one CTA.  Returns false when an
 // mbarrier wait timed out (the caller reports MPSB_ST_TIMEOUT); TMEM is
-// released on every path.
-template <int NT>
+// released on every path.  Called once per CTA (a CTA may allocate TMEM
+// only until it relinquishes the permit).  COHERENT: read the sites through
+// L2 (the dataflow kernel, where other clusters of the launch wrote them).
+template <int NT, bool COHERENT = false>
 __device__ bool contract_mixed(unsigned char *opbuf, uint64_t *mbar, uint32_t *tmem_slot, const double2 *A,
                                const double2 *B, const double2 *g, int cl, int cm, int cr, bool trans, int idx0,
                                int nidx, int C, int w, int wmax, int rpad, double2 *X, double2 *x0, int tid,
@@ -303,7 +313,7 @@ __device__ bool contract_mixed(unsigned char *opbuf, uint64_t *mbar, uint32_t *t
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
     for (int prod = 0; prod < 3; ++prod) {
-        stage_operands<NT>(opbuf, A, B, cl, cm, cr, trans, idx0, sh, prod, tid);
+        stage_operands<NT, COHERENT>(opbuf, A, B, cl, cm, cr, trans, idx0, sh, prod, tid);
         tc::fence_proxy_async();
         __syncthreads();
         if (tid == 0) {

@@ -28,6 +28,9 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <utility>
 
 namespace mpsb {
 
@@ -75,6 +78,9 @@ struct CtaScalars {
     int stamp[16];  // per column quad (slot * 8 + quad): rounds completed in the current step
     uint64_t mbar;            // tensor-core completion barrier (mixed form)
     uint32_t tmem;            // TMEM base address (mixed form)
+    int flow_item;            // dataflow form: the item this cluster claimed
+    int flow_slot;            // dataflow form: its workspace slot (-1: none)
+    int flow_skip;            // dataflow form: a wait gave up
 };
 static_assert(sizeof(CtaScalars) <= 384, "CTA scalars exceed their reserved header");
 
@@ -935,22 +941,39 @@ __device__ void form_rh(cg::cluster_group &cluster, const Slots &S, double2 *sta
 // chi_cap <= 16 (RPL = 1, ~13 KB shared) MPSB_RPL1_MIN_BLOCKS.
 template <int RPL, int NT>
 struct UpdMinBlocks {
-    static constexpr int value = RPL == 2 ? MPSB_RPL2_MIN_BLOCKS
+    static constexpr int value = RPL == 2 ? (NT == 128 ? MPSB_RPL2_MIN_BLOCKS : 1)
                                  : RPL == 1 ? (NT == 64 ? MPSB_RPL1_MIN_BLOCKS : MPSB_RPL1_MIN_BLOCKS / 2)
                                             : 1;
 };
 
-template <int RPL, int NT, bool MIXED>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RPL, NT>::value))
-    update2q_fp64_kernel(const Upd2Params p) {
+// A site element of the pair's input.  The per-layer kernel reads the sites
+// through the read-only path: within its launch no other CTA writes them.
+// The persistent kernel (FLOW) reads sites that CTAs of the same launch wrote
+// for earlier pairs, so it goes through L2, the coherence point (its waits on
+// those pairs end in acquire operations).
+template <bool FLOW>
+__device__ __forceinline__ double2 ld_site(const double2 *p) {
+    if constexpr (FLOW)
+        return __ldcg(p);
+    else
+        return __ldg(p);
+}
+
+// One two-site update by the calling cluster: pair `pr` (row `pi` of the
+// per-pair records), unrotated theta kept at x0 (this pair's workspace
+// region).  Both CTAs of the cluster call it with the same arguments; it ends
+// with a cluster barrier (or returns early, both CTAs together, for a pair
+// whose bond dimensions are out of range).  FLOW: the dataflow kernel's form,
+// which reads sites other clusters of the same launch wrote (through L2).
+template <int RPL, int NT, bool MIXED, bool FLOW>
+__device__ __forceinline__ void update_pair(const Upd2Params &p, const int pi, const mpsb_pair pr,
+                                            double2 *const x0pair, unsigned char *smem_raw) {
     constexpr int kUpdThreads = NT;
     constexpr int kUpdWarps = NT / 32;
     cg::cluster_group cluster = cg::this_cluster();
     const int crank = (int)cluster.block_rank();
-    const int pi = (int)(blockIdx.x >> 1);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     CtaScalars *sc = reinterpret_cast<CtaScalars *>(smem_raw);
     const int wmax = p.wmax, rpad = p.rpad;
     double2 *X = reinterpret_cast<double2 *>(smem_raw + 384);
@@ -964,7 +987,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
     QrScratch *qs = reinterpret_cast<QrScratch *>(smem_raw + upd_qr_offset(wmax, rpad));
     const Slots S{X, nrm, wmax, rpad};
 
-    const mpsb_pair pr = p.pairs[pi];
     const mpsb_chain ch = p.chains[pr.chain];
     const int i = pr.site;
     bool bad = (i < 0) || (i + 2 > ch.n);
@@ -1009,11 +1031,11 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
     if constexpr (MIXED) {
         const double2 *A = reinterpret_cast<const double2 *>(ch.sites + (size_t)i * ch.slot_elems);
         const double2 *B = reinterpret_cast<const double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
-        double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
+        double2 *x0 = x0pair;
         int nonfin = 0;
-        const bool ok = contract_mixed<NT>(reinterpret_cast<unsigned char *>(X), &sc->mbar, &sc->tmem, A, B,
-                                           sc->gate, cl, cm, cr, trans, idx0, nidx, C, w, wmax, rpad, X, x0, tid,
-                                           nonfin);
+        const bool ok = contract_mixed<NT, FLOW>(reinterpret_cast<unsigned char *>(X), &sc->mbar, &sc->tmem, A, B,
+                                                 sc->gate, cl, cm, cr, trans, idx0, nidx, C, w, wmax, rpad, X, x0,
+                                                 tid, nonfin);
         if (nonfin) atomicOr(&sc->nonfinite, 1);
         if (!ok && tid == 0) sc->timeout = 1;
         __threadfence();
@@ -1021,7 +1043,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
         const double2 *g = sc->gate;
         const double2 *A = reinterpret_cast<const double2 *>(ch.sites + (size_t)i * ch.slot_elems);
         const double2 *B = reinterpret_cast<const double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
-        double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
+        double2 *x0 = x0pair;
         const int other = trans ? cr : cl;
         const int total = nidx * other;
         int nonfin = 0;
@@ -1040,8 +1062,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
             const double2 *ap1 = ap0 + cm;
             const double2 *bp = B + d;
             for (int b = 0; b < cm; ++b) {
-                const double2 a0 = __ldg(ap0 + b), a1 = __ldg(ap1 + b);
-                const double2 b0 = __ldg(bp + (size_t)(2 * b) * cr), b1 = __ldg(bp + (size_t)(2 * b + 1) * cr);
+                const double2 a0 = ld_site<FLOW>(ap0 + b), a1 = ld_site<FLOW>(ap1 + b);
+                const double2 b0 = ld_site<FLOW>(bp + (size_t)(2 * b) * cr);
+                const double2 b1 = ld_site<FLOW>(bp + (size_t)(2 * b + 1) * cr);
                 t00 = c_fma(a0, b0, t00);
                 t01 = c_fma(a0, b1, t01);
                 t10 = c_fma(a1, b0, t10);
@@ -1083,7 +1106,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
     // converge in a few sweeps.
     bool precond = w >= 8 && (w >> 1) <= 2 * kUpdWarps;
     if (precond) {
-        const double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
+        const double2 *x0 = x0pair;
         precond = qr_sort_reload<RPL, NT>(cluster, S, sig2, qs, crank, w, R, C, cr, trans, x0, warp, lane, tid);
         if (precond) {
             qr_factor<RPL, NT>(cluster, S, stage, qs, crank, w, C, warp, lane);
@@ -1238,7 +1261,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
             else
                 Aout[(size_t)col * K + rho] = c_scale(v, f);
         }
-        const double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
+        const double2 *x0 = x0pair;
         constexpr int kRows = NT < 128 ? NT : 128;  // threads per row group
         constexpr int kGroups = NT / kRows;
         const int grp = tid / kRows;
@@ -1288,7 +1311,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
         }
         // other side: Y[rho, col] = sum_r conj(x_j[r]) X0[r, col]
         {
-            const double2 *x0 = p.x0 + (size_t)pi * p.x0_stride;
+            const double2 *x0 = x0pair;
             constexpr int kCols = NT < 128 ? NT : 128;  // threads per column group
             constexpr int kGroups = NT / kCols;
             const int grp = tid / kCols;
@@ -1358,6 +1381,153 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RP
     }
     if (crank == 0 && tid == 0) ch.bonds[i + 1] = K;
     cluster.sync();
+}
+
+// One launch = one layer: cluster c updates pair c.
+template <int RPL, int NT, bool MIXED>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RPL, NT>::value))
+    update2q_fp64_kernel(const Upd2Params p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int pi = (int)(blockIdx.x >> 1);
+    update_pair<RPL, NT, MIXED, false>(p, pi, p.pairs[pi], p.x0 + (size_t)pi * p.x0_stride, smem_raw);
+}
+
+// ------------------------------------------------------------- dataflow form
+// One launch for a whole program of updates (many layers of many chains): the
+// grid has one two-CTA cluster per item of a work list, and every cluster, as
+// the hardware starts it, claims the next unclaimed item with one atomic add
+// -- so items are taken in list order, whatever order the clusters start in
+// -- then waits until the items it depends on (the last earlier items that
+// touched its two sites) have finished.  A pair of layer L+1 thus starts as
+// soon as its two neighbours of layer L are done, while unrelated pairs of
+// layer L are still running: no launch boundary, no per-layer tail.  The list
+// is in topological order (every dependency precedes its item) and only
+// running clusters hold claims, so the lowest unfinished claimed item always
+// has its dependencies finished: the launch always progresses.  Every wait is
+// bounded: after poll_limit polls the item is skipped with MPSB_ST_TIMEOUT
+// (its sites stay as they were) and still marked finished.  The per-pair work
+// is the per-layer kernel's own body, inlined the same way (a persistent loop
+// around it, or a call to it, made ptxas spill 2-4 KB per thread).  The
+// unrotated-theta copies live in a pool of one slot per resident cluster.
+struct FlowParams {
+    const mpsb_flow_item *items;
+    int nitems;
+    int *claim;        // next unclaimed item (zeroed before the launch)
+    int *done;         // per item: 1 once finished (zeroed before the launch)
+    int *slot_busy;    // per workspace slot: 1 while a cluster holds it (zeroed before the launch)
+    int nslots;
+    int poll_limit;
+};
+
+__device__ __forceinline__ int ld_acquire_gpu(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int *p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Bounded wait for item dep (dep < 0: none) to finish; false when it gave up
+// (or when dep is not an item of the list).
+__device__ __forceinline__ bool wait_done(const int *done, int dep, int nitems, int limit) {
+    if (dep < 0) return true;
+    if (dep >= nitems) return false;
+    for (int polls = 0;; ++polls) {
+        if (ld_acquire_gpu(done + dep)) return true;
+        if (polls >= limit) return false;
+        __nanosleep(128);
+    }
+}
+
+// A free workspace slot (bounded search; -1 when none turned up).  Slot
+// holders only wait on items claimed by other slot holders, which run, so a
+// slot always frees up; with as many slots as clusters can be resident the
+// search succeeds at once.
+__device__ __forceinline__ int take_slot(int *busy, int nslots, int start, int limit) {
+    const int rounds = limit / nslots;  // about `limit` probes in all
+    for (int round = 0; round <= rounds; ++round) {
+        for (int j = 0; j < nslots; ++j) {
+            const int s = (start + j) % nslots;
+            if (atomicCAS(busy + s, 0, 1) == 0) return s;
+        }
+        __nanosleep(128);
+    }
+    return -1;
+}
+
+template <int RPL, int NT, bool MIXED>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(NT, (UpdMinBlocks<RPL, NT>::value))
+    update2q_flow_kernel(const Upd2Params p, const FlowParams f) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int crank = (int)cluster.block_rank();
+    const int tid = threadIdx.x;
+    CtaScalars *sc = reinterpret_cast<CtaScalars *>(smem_raw);
+    cluster.sync();  // both CTAs running before the distributed shared-memory stores
+    if (crank == 0 && tid == 0) {
+        // slot first, claim second: a cluster still looking for a slot holds
+        // no claim that another cluster could be waiting on
+        const int slot = take_slot(f.slot_busy, f.nslots, (int)(blockIdx.x >> 1) % f.nslots, f.poll_limit);
+        const int k = atomicAdd(f.claim, 1);
+        sc->flow_item = k;
+        sc->flow_slot = slot;
+        *cluster.map_shared_rank(&sc->flow_item, 1) = k;
+        *cluster.map_shared_rank(&sc->flow_slot, 1) = slot;
+    }
+    cluster.sync();
+    const int k = sc->flow_item, slot = sc->flow_slot;
+    if (k >= f.nitems) {  // only when the grid exceeds the list
+        if (crank == 0 && tid == 0 && slot >= 0) atomicExch(f.slot_busy + slot, 0);
+        return;
+    }
+    const mpsb_flow_item it = f.items[k];
+    // each CTA acquires the producers' writes for its own SM
+    if (tid == 0)
+        sc->flow_skip = slot < 0 || !(wait_done(f.done, it.dep0, f.nitems, f.poll_limit) &&
+                                      wait_done(f.done, it.dep1, f.nitems, f.poll_limit));
+    cluster.sync();
+    const int skip = sc->flow_skip | *cluster.map_shared_rank(&sc->flow_skip, crank ^ 1);
+    fence_acq_rel_gpu();
+    if (!skip) {
+        update_pair<RPL, NT, MIXED, true>(p, k, mpsb_pair{it.chain, it.site, it.gate, it.out},
+                                          p.x0 + (size_t)slot * p.x0_stride, smem_raw);
+    } else if (crank == 0 && tid == 0) {
+        const mpsb_chain ch = p.chains[it.chain];
+        const int cm = (it.site >= 0 && it.site + 2 <= ch.n) ? ch.bonds[it.site + 1] : 0;
+        p.rec[k] = PairRec{0.0, 0.0, 0.0, cm, MPSB_ST_TIMEOUT};
+        p.status[it.out] = MPSB_ST_TIMEOUT;
+        if (p.kept) p.kept[it.out] = cm;
+        if (p.trunc) p.trunc[it.out] = 0.0;
+    }
+    __threadfence();
+    cluster.sync();  // both CTAs done with item k and with the slot
+    if (crank == 0 && tid == 0) {
+        if (slot >= 0) atomicExch(f.slot_busy + slot, 0);
+        st_release_gpu(f.done + k, 1);
+    }
+}
+
+// Fold of the persistent form: chain c's items are order[off[c] .. off[c+1])
+// in application order.
+__global__ void fold_flow_kernel(const mpsb_chain *chains, int nchains, const int32_t *order, const int32_t *off,
+                                 const PairRec *rec) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nchains) return;
+    const int b = off[c], e = off[c + 1];
+    if (e <= b) return;
+    double *nl = chains[c].norm_log;
+    double acc = *nl;
+    int st = 0;
+    for (int q = b; q < e; ++q) {
+        const PairRec r = rec[order[q]];
+        acc += r.d_trunc;
+        acc += r.d_norm;
+        st |= r.status;
+    }
+    *nl = acc;
+    if (chains[c].status_acc && st) atomicOr(chains[c].status_acc, st);
 }
 
 // Fold per-pair norm_log increments into each chain, in pair order
@@ -1477,6 +1647,170 @@ int launch_update2q_mixed(const mpsb_chain *chains, const mpsb_pair *pairs, int 
                           double *trunc, int32_t *status, cudaStream_t stream) {
     return launch_update2q_impl(true, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
                                 trunc, status, stream);
+}
+
+// ------------------------------------------------------- persistent launcher
+namespace {
+
+// The CTA shape of a launch: rows per lane from the bond cap, threads from
+// the caller (0 = the per-layer kernel's choice), tensor cores only at
+// chi_cap > 32 for the mixed form.
+struct FlowShape {
+    int rpl, nt;
+    bool mixed;
+    size_t smem;
+};
+
+int flow_shape(int chi_cap, int precision, int threads, FlowShape &sh) {
+    sh.rpl = (2 * chi_cap <= 32) ? 1 : (2 * chi_cap <= 64) ? 2 : 4;
+    const int deflt = sh.rpl == 1 ? 64 : sh.rpl == 2 ? 128 : kUpdThreads;
+    sh.nt = threads <= 0 ? deflt : threads;
+    const bool ok = (sh.rpl == 1 && (sh.nt == 64 || sh.nt == 128)) || (sh.rpl == 2 && (sh.nt == 128 || sh.nt == 256)) ||
+                    (sh.rpl == 4 && sh.nt == 256);
+    if (!ok) return set_error(MPSB_EINVAL, "threads=%d is not a CTA shape for chi_cap=%d", threads, chi_cap);
+    sh.mixed = precision == MPSB_MIXED_TF32X3 && sh.rpl == 4;
+    const int wmax = (((2 * chi_cap) + 15) & ~15) / 4, rpad = 32 * sh.rpl;
+    sh.smem = sh.mixed ? upd_smem_bytes_mixed(wmax, rpad, chi_cap) : upd_smem_bytes(wmax, rpad);
+    return MPSB_OK;
+}
+
+const void *flow_kernel_ptr(const FlowShape &sh) {
+    if (sh.mixed) return reinterpret_cast<const void *>(update2q_flow_kernel<4, kUpdThreads, true>);
+    if (sh.rpl == 1)
+        return sh.nt == 64 ? reinterpret_cast<const void *>(update2q_flow_kernel<1, 64, false>)
+                           : reinterpret_cast<const void *>(update2q_flow_kernel<1, 128, false>);
+    if (sh.rpl == 2)
+        return sh.nt == 128 ? reinterpret_cast<const void *>(update2q_flow_kernel<2, 128, false>)
+                            : reinterpret_cast<const void *>(update2q_flow_kernel<2, 256, false>);
+    return reinterpret_cast<const void *>(update2q_flow_kernel<4, kUpdThreads, false>);
+}
+
+// Two-CTA clusters of this shape resident at once on the current device
+// (remembered per kernel and device).
+int flow_max_clusters(const FlowShape &sh, int &out) {
+    const void *fn = flow_kernel_ptr(sh);
+    int rc = ensure_smem(fn, sh.smem, "cudaFuncSetAttribute(update2q flow)");
+    if (rc) return rc;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_error(MPSB_ENODEV, "no CUDA device");
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> known;
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(fn, dev);
+    auto hit = known.find(key);
+    if (hit != known.end()) {
+        out = hit->second;
+        return MPSB_OK;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2, 1, 1);
+    cfg.blockDim = dim3(sh.nt, 1, 1);
+    cfg.dynamicSmemBytes = sh.smem;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess || n < 1)
+        return check_launch("cudaOccupancyMaxActiveClusters(update2q flow)");
+    known[key] = n;
+    out = n;
+    return MPSB_OK;
+}
+
+// Workspace of the dataflow form: [claim counter | done flags | slot flags]
+// (zeroed per launch), then per-item records and `nslots` theta copies.
+size_t flow_flag_bytes(int nitems, int nslots) {
+    return 256 + align256((size_t)nitems * sizeof(int)) + align256((size_t)nslots * sizeof(int));
+}
+size_t flow_ws_bytes(int nitems, int chi_cap, int nslots) {
+    const size_t x0_stride = (size_t)(2 * chi_cap) * (2 * chi_cap);
+    return flow_flag_bytes(nitems, nslots) + align256((size_t)nitems * sizeof(PairRec)) +
+           (size_t)nslots * x0_stride * sizeof(double2);
+}
+
+template <int RPL, int NT, bool MIXED>
+int launch_flow_rpl(const Upd2Params &p, const FlowParams &f, size_t smem, cudaStream_t s) {
+    update2q_flow_kernel<RPL, NT, MIXED><<<2 * f.nitems, NT, smem, s>>>(p, f);
+    return check_launch("update2q flow kernel");
+}
+
+}  // namespace
+
+size_t upd_flow_workspace_bytes(int nitems, int chi_cap, int precision, int threads, int nclusters) {
+    if (nclusters <= 0) {
+        FlowShape sh;
+        if (flow_shape(chi_cap, precision, threads, sh) != MPSB_OK || flow_max_clusters(sh, nclusters) != MPSB_OK)
+            return 0;
+    }
+    return flow_ws_bytes(nitems, chi_cap, nclusters);
+}
+
+int upd_flow_clusters(int chi_cap, int precision, int threads) {
+    FlowShape sh;
+    int n = 0;
+    int rc = flow_shape(chi_cap, precision, threads, sh);
+    if (rc) return rc;
+    rc = flow_max_clusters(sh, n);
+    return rc ? rc : n;
+}
+
+int launch_update2q_flow(const mpsb_chain *chains, int nchains, const mpsb_flow_item *items, int nitems,
+                         const int32_t *order, const int32_t *offsets, const double2 *gates, int precision,
+                         int chi_cap, double tol, int max_sweeps, int threads, int nclusters, int poll_limit,
+                         void *ws, size_t ws_bytes, double *spectra, int32_t *kept, double *trunc, int32_t *status,
+                         cudaStream_t stream) {
+    if (nitems == 0) return MPSB_OK;
+    FlowShape sh;
+    int rc = flow_shape(chi_cap, precision, threads, sh);
+    if (rc) return rc;
+    int most = 0;
+    rc = flow_max_clusters(sh, most);
+    if (rc) return rc;
+    if (nclusters <= 0 || nclusters > most) nclusters = most;
+    if (nclusters > nitems) nclusters = nitems;
+    const size_t need = flow_ws_bytes(nitems, chi_cap, nclusters);
+    if (ws_bytes < need) return set_error(MPSB_EWORKSPACE, "flow workspace of %zu bytes < %zu needed", ws_bytes, need);
+    char *w = static_cast<char *>(ws);
+    const size_t flags = flow_flag_bytes(nitems, nclusters);
+    FlowParams f;
+    f.items = items;
+    f.nitems = nitems;
+    f.claim = reinterpret_cast<int *>(w);
+    f.done = reinterpret_cast<int *>(w + 256);
+    f.slot_busy = reinterpret_cast<int *>(w + 256 + align256((size_t)nitems * sizeof(int)));
+    f.nslots = nclusters;
+    f.poll_limit = poll_limit < 0 ? (1 << 24) : poll_limit;
+    Upd2Params p;
+    p.chains = chains;
+    p.pairs = nullptr;
+    p.npairs = nitems;
+    p.gates = gates;
+    p.rec = reinterpret_cast<PairRec *>(w + flags);
+    p.x0 = reinterpret_cast<double2 *>(w + flags + align256((size_t)nitems * sizeof(PairRec)));
+    p.x0_stride = (long long)(2 * chi_cap) * (2 * chi_cap);
+    p.tape_xs = nullptr;
+    p.tape_meta = nullptr;
+    p.spectra = spectra;
+    p.kept = kept;
+    p.trunc = trunc;
+    p.status = status;
+    p.chi_cap = chi_cap;
+    p.rpad = 32 * sh.rpl;
+    p.wmax = (((2 * chi_cap) + 15) & ~15) / 4;
+    p.tol2 = tol * tol;
+    p.max_sweeps = max_sweeps;
+    p.cut_floor = sh.mixed ? kMixedCutoffFloor : 0.0;
+    if (cudaMemsetAsync(w, 0, flags, stream) != cudaSuccess) return check_launch("cudaMemsetAsync(flow flags)");
+    if (sh.mixed)
+        rc = launch_flow_rpl<4, kUpdThreads, true>(p, f, sh.smem, stream);
+    else if (sh.rpl == 1)
+        rc = sh.nt == 64 ? launch_flow_rpl<1, 64, false>(p, f, sh.smem, stream)
+                         : launch_flow_rpl<1, 128, false>(p, f, sh.smem, stream);
+    else if (sh.rpl == 2)
+        rc = sh.nt == 128 ? launch_flow_rpl<2, 128, false>(p, f, sh.smem, stream)
+                          : launch_flow_rpl<2, 256, false>(p, f, sh.smem, stream);
+    else
+        rc = launch_flow_rpl<4, kUpdThreads, false>(p, f, sh.smem, stream);
+    if (rc) return rc;
+    fold_flow_kernel<<<(nchains + 127) / 128, 128, 0, stream>>>(chains, nchains, order, offsets, p.rec);
+    return check_launch("fold_flow_kernel");
 }
 
 int launch_update2q_taped(bool mixed, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,

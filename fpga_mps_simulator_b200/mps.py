@@ -31,7 +31,8 @@ import torch
 from . import _lib
 from .gates import GATE_MATRICES, permute_2q
 
-__all__ = ["MPSState", "MPSBatch", "PairBatch", "PRECISIONS", "validate_pairs", "overlap", "infidelity"]
+__all__ = ["MPSState", "MPSBatch", "PairBatch", "FlowBatch", "PRECISIONS", "validate_pairs", "flow_items", "overlap",
+           "infidelity"]
 
 PRECISIONS = {"fp64": _lib.FP64, "complex128": _lib.FP64, "mixed": _lib.MIXED_TF32X3,
               "tf32x3": _lib.MIXED_TF32X3}
@@ -73,6 +74,40 @@ def validate_pairs(ns: Sequence[int], chain_idx: np.ndarray, sites: np.ndarray) 
     same = cs[1:] == cs[:-1]
     if np.any(same & (ss[1:] - ss[:-1] < 2)):
         raise ValueError("pairs of one launch must be disjoint")
+
+
+def flow_items(ns: Sequence[int], chain_idx, sites) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Work list of the dataflow update launch from updates listed in application order.
+
+    Item k is the update (chain_idx[k], sites[k]); a chain's updates apply in
+    the order they appear.  Returns (items, order, offsets): items (K, 6) int32
+    rows (chain, site, gate = k, out = k, dep0, dep1) where dep0 / dep1 are
+    the last earlier items touching site i / site i+1 of the same chain (-1:
+    none), so every dependency precedes its item (the topological order the
+    kernel's forward progress rests on); order / offsets list each chain's
+    items (CSR, chain c at order[offsets[c]:offsets[c+1]]) for the per-chain
+    norm_log fold.
+    """
+    chain_idx = np.asarray(chain_idx, np.int64).reshape(-1)
+    sites = np.asarray(sites, np.int64).reshape(-1)
+    if len(chain_idx) != len(sites):
+        raise ValueError("chain_idx and sites differ in length")
+    K = len(sites)
+    if K and (np.any(chain_idx < 0) or np.any(chain_idx >= len(ns))):
+        raise ValueError("item chain index out of range")
+    if K and (np.any(sites < 0) or np.any(sites + 1 >= np.asarray(ns, np.int64)[chain_idx])):
+        raise ValueError("item site out of range: need 0 <= i and i + 1 < n")
+    items = np.empty((K, 6), np.int32)
+    last: Dict[Tuple[int, int], int] = {}
+    for k in range(K):
+        c, i = int(chain_idx[k]), int(sites[k])
+        items[k] = (c, i, k, k, last.get((c, i), -1), last.get((c, i + 1), -1))
+        last[(c, i)] = k
+        last[(c, i + 1)] = k
+    order = np.argsort(chain_idx, kind="stable").astype(np.int32)
+    offsets = np.zeros(len(ns) + 1, np.int32)
+    np.cumsum(np.bincount(chain_idx, minlength=len(ns)), out=offsets[1:])
+    return items, order, offsets
 
 
 class _Workspace:
@@ -126,6 +161,44 @@ class PairBatch:
     def set_gates(self, gates: np.ndarray) -> None:
         g = torch.from_numpy(np.ascontiguousarray(np.asarray(gates, np.complex128).reshape(self.npairs, 16)))
         self.gates.copy_(g, non_blocking=False)
+
+
+class FlowBatch:
+    """Device work list for one dataflow launch: many layers of many chains.
+
+    ``chain_idx``, ``sites``, ``gates`` list updates in application order
+    (e.g. layer by layer); outputs (status, kept, trunc, spectra) have one row
+    per item.  Reusable across launches and CUDA-graph replays.
+    """
+
+    def __init__(self, owner: "MPSBatch", chain_idx, sites, gates, record_spectra: bool = False):
+        items, order, offsets = flow_items(owner.ns, chain_idx, sites)
+        dev = owner.device
+        self.owner = owner
+        self.nitems = len(items)
+        self.items = torch.from_numpy(np.ascontiguousarray(items)).to(dev)
+        self.order = torch.from_numpy(order).to(dev)
+        self.offsets = torch.from_numpy(offsets).to(dev)
+        self.gates = torch.empty(self.nitems, 16, dtype=torch.complex128, device=dev)
+        self.set_gates(gates)
+        self.status = torch.zeros(self.nitems, dtype=torch.int32, device=dev)
+        self.kept = torch.zeros(self.nitems, dtype=torch.int32, device=dev)
+        self.trunc = torch.zeros(self.nitems, dtype=torch.float64, device=dev)
+        self.spectra = torch.zeros(self.nitems, 128, dtype=torch.float64, device=dev) if record_spectra else None
+        self.host_items = items
+
+    def set_gates(self, gates) -> None:
+        """Replace the gates (one 4x4 per item, list order): a numpy array, or a
+        torch tensor -- from pinned host memory the copy is asynchronous."""
+        if isinstance(gates, torch.Tensor):
+            if gates.dtype != torch.complex128 or gates.numel() != 16 * self.nitems:
+                raise ValueError("gates must be complex128 with one 4x4 per item")
+            self.gates.copy_(gates.reshape(self.nitems, 16), non_blocking=True)
+            return
+        g = np.asarray(gates, dtype=np.complex128)
+        if g.size != 16 * self.nitems:
+            raise ValueError("need one gate per item")
+        self.gates.copy_(torch.from_numpy(np.ascontiguousarray(g.reshape(self.nitems, 16))))
 
 
 class MPSBatch:
@@ -243,6 +316,35 @@ class MPSBatch:
             cap, self.tol, self.max_sweeps, ws.data_ptr(), ws.numel(),
             _ptr(pb.spectra), pb.kept.data_ptr(), pb.trunc.data_ptr(), pb.status.data_ptr(), handle)
         _lib.check(rc, "mpsb_update2q_batch")
+
+    def make_flow(self, chain_idx, sites, gates, record_spectra: bool = False) -> FlowBatch:
+        return FlowBatch(self, chain_idx, sites, gates, record_spectra)
+
+    def run_flow(self, fb: FlowBatch, precision: Optional[str] = None, chi_cap: Optional[int] = None,
+                 threads: int = 0, nclusters: int = 0, poll_limit: int = -1,
+                 workspace: Optional[_Workspace] = None, stream: Optional[torch.cuda.Stream] = None) -> None:
+        """One dataflow launch over the whole work list (asynchronous, graph-capturable).
+
+        ``threads`` picks the CTA shape (0 = default for the cap), ``nclusters``
+        the number of workspace slots, i.e. concurrently working clusters
+        (0 = all that fit), ``poll_limit`` the polls per dependency wait
+        (-1 = the library default).
+        """
+        if fb.nitems == 0:
+            return
+        prec = PRECISIONS[precision or self.precision]
+        cap = self.chi_cap if chi_cap is None else int(chi_cap)
+        need = self._lib.mpsb_update2q_flow_workspace_bytes(fb.nitems, cap, prec, int(threads), int(nclusters))
+        if need == 0:
+            _lib.check(-1, "mpsb_update2q_flow_workspace_bytes")
+        ws = (workspace or self._ws).get(need)
+        handle = (stream or torch.cuda.current_stream(self.device)).cuda_stream
+        rc = self._lib.mpsb_update2q_flow(
+            self.table.data_ptr(), self.nchains, fb.items.data_ptr(), fb.nitems, fb.order.data_ptr(),
+            fb.offsets.data_ptr(), fb.gates.data_ptr(), prec, cap, self.tol, self.max_sweeps, int(threads),
+            int(nclusters), int(poll_limit), ws.data_ptr(), ws.numel(), _ptr(fb.spectra), fb.kept.data_ptr(),
+            fb.trunc.data_ptr(), fb.status.data_ptr(), handle)
+        _lib.check(rc, "mpsb_update2q_flow")
 
     def snapshot(self):
         """Device copies of the mutable state (sites, bonds, norm_log, status)."""
@@ -599,6 +701,32 @@ class MPSState:
         self.last_pairs = self._b.apply_layer(np.zeros(len(sites), np.int32), sites, gates,
                                               record_spectra=record_spectra)
         return self.last_pairs
+
+    def apply_layers(self, layer_sites: Sequence[Sequence[int]], gates,
+                     flow: Optional[FlowBatch] = None) -> FlowBatch:
+        """Many layers of adjacent pairs in ONE dataflow launch.
+
+        ``layer_sites[L]`` lists the left sites of layer L; ``gates`` holds one
+        4x4 per pair in layer order (numpy, or a torch tensor, e.g. in pinned
+        host memory).  Updates apply in that order -- the result is
+        bit-identical to ``apply_layer`` for each layer in turn -- but each
+        pair starts as soon as the two updates before it on its sites are
+        done.  Passing the FlowBatch a previous call returned (same layers)
+        reuses its device tables and only copies the new gates.
+        """
+        if flow is None:
+            sites = np.concatenate([np.asarray(s, np.int32).reshape(-1) for s in layer_sites]) \
+                if len(layer_sites) else np.zeros(0, np.int32)
+            for s in layer_sites:  # each layer disjoint, as a layer of apply_layer must be
+                validate_pairs([self.n], np.zeros(len(s), np.int64), np.asarray(s, np.int64))
+            flow = self._b.make_flow(np.zeros(len(sites), np.int32), sites,
+                                     np.zeros((len(sites), 4, 4), np.complex128))
+        if flow.owner is not self._b:
+            raise ValueError("the flow belongs to another state")
+        flow.set_gates(gates)
+        self._b.run_flow(flow)
+        self.last_flow = flow
+        return flow
 
     # -- read-out ------------------------------------------------------------
     def get_statevector(self) -> np.ndarray:

@@ -72,6 +72,15 @@ typedef struct {
     int32_t out;    /* row of this pair in status / kept / trunc / spectra  */
 } mpsb_pair;
 
+/* One two-site update of a dependency-ordered work list (mpsb_update2q_flow):
+ * the fields of mpsb_pair, then the list indices of the two items it must
+ * wait for -- the last earlier items touching site `site` and site `site + 1`
+ * of the same chain -- or -1 where there is none.  dep0, dep1 < own index. */
+typedef struct {
+    int32_t chain, site, gate, out;
+    int32_t dep0, dep1;
+} mpsb_flow_item;
+
 /* One single-site gate: 2x2 gate `gate` on site `site` of chain `chain`. */
 typedef struct {
     int32_t chain;
@@ -158,6 +167,39 @@ MPSB_API int mpsb_update2q_batch_noalloc(const mpsb_chain *chains, const mpsb_pa
                                          double tol, int max_sweeps,
                                          double *spectra, int32_t *kept, double *trunc, int32_t *status,
                                          mpsb_stream_t stream);
+
+/* Persistent dataflow form of mpsb_update2q_batch: many layers of many
+ * chains in ONE launch.  A grid of `nclusters` resident two-CTA clusters
+ * claims the items in list order; an item starts as soon as its dep0 / dep1
+ * items have finished (bounded waits: after poll_limit polls the item is
+ * skipped, its sites unchanged, with MPSB_ST_TIMEOUT), so a pair of layer
+ * L + 1 runs while unrelated pairs of layer L are still in flight.  Every
+ * item computes exactly what mpsb_update2q_batch computes for it (same
+ * per-pair code): sites, bonds, spectra, kept counts and statuses are
+ * bit-identical to launching the layers one by one.
+ *   items: device, nitems, in topological order (each dep < its own index).
+ *   chain_order, chain_offsets: device; chain c's items, in the order they
+ *     apply, are chain_order[chain_offsets[c] .. chain_offsets[c+1]); norm_log
+ *     is folded per chain in that order (as per-layer launches fold it).
+ *   threads: CTA size (0 = default; 64 or 128 at chi_cap <= 16, 128 or 256
+ *     at chi_cap <= 32, 256 above) -- the shape the autotuner chooses.
+ *   nclusters: grid size (<= 0 = every cluster that fits on the current device).
+ *   poll_limit: polls per dependency wait before giving up (< 0 = 2^24).
+ *   workspace: mpsb_update2q_flow_workspace_bytes(nitems, chi_cap, precision,
+ *     threads, nclusters) bytes, 256-byte aligned.
+ * Launches two memsets, the persistent kernel and a fold kernel.  No reference
+ * counterpart: replaces the host loop over gates of fpga_mps_simulator.py:566-635
+ * (one launch and one host round trip per gate). */
+MPSB_API size_t mpsb_update2q_flow_workspace_bytes(int nitems, int chi_cap, int precision, int threads,
+                                                   int nclusters);
+MPSB_API int mpsb_update2q_flow_clusters(int chi_cap, int precision, int threads);
+MPSB_API int mpsb_update2q_flow(const mpsb_chain *chains, int nchains, const mpsb_flow_item *items, int nitems,
+                                const int32_t *chain_order, const int32_t *chain_offsets,
+                                const mpsb_c128 *gates, int precision, int chi_cap, double tol, int max_sweeps,
+                                int threads, int nclusters, int poll_limit,
+                                void *workspace, size_t workspace_bytes,
+                                double *spectra, int32_t *kept, double *trunc, int32_t *status,
+                                mpsb_stream_t stream);
 
 /* Batched single-site gates, A'[l,s',r] = sum_s G[s',s] A[l,s,r], in place
  * (mps_core.py:267-273; fpga_mps_simulator.cpp:232-276 apply_1q_gate).
@@ -268,7 +310,8 @@ MPSB_API int mpsb_update2q_batch_taped(const mpsb_chain *chains, const mpsb_pair
                                        double *spectra, int32_t *kept, double *trunc, int32_t *status,
                                        mpsb_stream_t stream);
 
-/* Bytes of device workspace mpsb_update2q_backward_batch needs: one scratch
+/* Bytes of device workspace mpsb_update2q_backward_batch needs (256-byte
+ * aligned; each pair's dead scratch is dropped from L2 unwritten): one scratch
  * region of 8 (2 chi_cap)^2 complex per CTA, min(npairs, CTAs resident on the
  * current device).  Call with the device of the launch current. */
 MPSB_API size_t mpsb_update2q_backward_workspace_bytes(int npairs, int chi_cap);

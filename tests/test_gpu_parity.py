@@ -236,7 +236,8 @@ def test_nonfinite_gate_is_reported():
 def test_bad_arguments_raise():
     from fpga_mps_simulator_b200 import MPSState
     with pytest.raises(ValueError):
-        MPSState(4, 65)
+        MPSState(4, 0)
+    assert MPSState(4, 65).chi_max == 65  # any cap >= 1; the device limit is reported per update
     st = MPSState(6, 8)
     with pytest.raises(ValueError, match="disjoint"):
         st.apply_layer([0, 1], np.stack([np.eye(4)] * 2))

@@ -33,7 +33,7 @@ def _batch(specs, precision, cutoff):
     return MPSBatch([s.n for s in specs], [s.chi_max for s in specs], cutoff, precision=precision)
 
 
-@pytest.mark.parametrize("strategy", ["single", "lpt", "split"])
+@pytest.mark.parametrize("strategy", ["single", "lpt", "split", "flow"])
 def test_strategies_match_oracle(strategy):
     from fpga_mps_simulator_b200.schedule import Runner, Schedule
     specs = _specs()
@@ -48,7 +48,7 @@ def test_strategies_match_oracle(strategy):
         np.testing.assert_allclose(b.statevector(c), sv, rtol=0, atol=TOL * np.max(np.abs(sv)))
 
 
-@pytest.mark.parametrize("strategy", ["lpt", "split"])
+@pytest.mark.parametrize("strategy", ["lpt", "split", "flow"])
 def test_graph_replay_is_bitwise_eager(strategy):
     from fpga_mps_simulator_b200.schedule import Runner, Schedule
     specs = _specs()

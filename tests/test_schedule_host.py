@@ -33,6 +33,48 @@ class _FakeBatch:
         return _FakePairs(self.ns, ci, si, gates)
 
 
+def test_flow_items_dependencies_are_the_last_earlier_touch():
+    from fpga_mps_simulator_b200.mps import flow_items
+    # chain 0 (n=6): (0,1) (2,3) (4,5) | (1,2) (3,4) ; chain 1 (n=4): (0,1) (2,3) | (1,2)
+    ci = [0, 0, 0, 1, 1, 0, 0, 1]
+    si = [0, 2, 4, 0, 2, 1, 3, 1]
+    items, order, off = flow_items([6, 4], ci, si)
+    assert items[:, 2].tolist() == list(range(8)) and items[:, 3].tolist() == list(range(8))
+    deps = {k: (int(items[k, 4]), int(items[k, 5])) for k in range(8)}
+    assert deps[0] == deps[1] == deps[2] == deps[3] == deps[4] == (-1, -1)
+    assert deps[5] == (0, 1) and deps[6] == (1, 2) and deps[7] == (3, 4)
+    assert all(d < k for k, ds in deps.items() for d in ds)  # topological
+    assert off.tolist() == [0, 5, 8]
+    assert order[:5].tolist() == [0, 1, 2, 5, 6] and order[5:].tolist() == [3, 4, 7]
+    with pytest.raises(ValueError, match="range"):
+        flow_items([6], [0], [5])
+
+
+def test_flow_plan_lists_each_class_layer_by_layer(specs):
+    class _Fake(_FakeBatch):
+        def make_flow(self, ci, si, gates, record_spectra=False):
+            from fpga_mps_simulator_b200.mps import flow_items
+            flow_items(self.ns, ci, si)
+            return _FakePairs.__new__(_FakePairs), (list(ci), list(si), np.asarray(gates))
+
+    b = _Fake(specs)
+    sch = Schedule(b, [s.layers for s in specs])
+    plan = sch.flow_plan()
+    assert [fl.chi_cap for fl in plan] == sorted(set(b.caps), reverse=True)
+    total = 0
+    for fl in plan:
+        ci, si, gates = fl.fb[1]
+        total += len(ci)
+        assert {b.caps[c] for c in ci} == {fl.chi_cap}
+        for c in set(ci):  # a chain's updates in layer order, each layer in its own order
+            mine = [(s, g) for cc, s, g in zip(ci, si, gates) if cc == c]
+            want = [(int(i), g) for L in specs[c].layers for i, g in zip(L.sites, L.gates)]
+            assert [s for s, _ in mine] == [s for s, _ in want]
+            for (_, g1), (_, g2) in zip(mine, want):
+                np.testing.assert_array_equal(g1, g2)
+    assert total == sch.updates()
+
+
 @pytest.fixture(scope="module")
 def specs():
     return random_circuit_batch(24, seed=5, n_range=(6, 40), depth_range=(2, 9), chis=(4, 16, 64))
