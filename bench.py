@@ -45,8 +45,9 @@ WORKLOAD = (f"MPS two-site updates: n={N_SITES} open chain, depth-{DEPTH} Haar b
 
 
 # DRAM bytes (read + write) of one dataflow launch (the whole 990-update step,
-# mixed form), from one ncu capture of this workload; None until measured.
-TRAFFIC_PER_LAUNCH = None
+# mixed form), from one ncu capture of this workload: 1.15 MB read + 3.36 MB
+# written (sites and theta copies stay in L2).
+TRAFFIC_PER_LAUNCH = 4.51e6
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one dataflow launch of this "
                   "workload (990 updates); algorithmic site bytes per step in hbm_site_bytes_per_step")
 
@@ -231,7 +232,7 @@ def gradient_leg(dev, steps: int, warmup: int, rank: int, max_over_ranks, cpu_wo
     angles = torch.tensor(hea_angles(GRAD_N, GRAD_LAYERS, GRAD_VEC, SEED + rank), dtype=torch.float64, device=dev)
     out, grads, finals = {}, {}, {}
     flops = None
-    for prec, ckpt in (("fp64", "auto"), ("mixed", "auto"), ("fp64", True)):
+    for prec, ckpt in (("fp64", "auto"), ("mixed", "auto"), ("mixed_all", "auto"), ("fp64", True)):
         model = HEAEnergy(GRAD_N, GRAD_LAYERS, GRAD_VEC, chi_max=GRAD_CHI, cutoff=GRAD_CUT, precision=prec,
                           device=dev, checkpoint=ckpt)
         for _ in range(warmup):
@@ -262,32 +263,40 @@ def gradient_leg(dev, steps: int, warmup: int, rank: int, max_over_ranks, cpu_wo
         del model
         torch.cuda.empty_cache()
     from fpga_mps_simulator_b200.mps import overlap
-    infid = []
-    for c in range(GRAD_VEC):  # final ansatz states, mixed vs FP64 form
-        ab, lab = overlap(finals["mixed"], c, finals["fp64"], c)
-        aa, laa = overlap(finals["mixed"], c, finals["mixed"], c)
-        bb, lbb = overlap(finals["fp64"], c, finals["fp64"], c)
-        infid.append(1.0 - abs(ab) ** 2 / (aa.real * bb.real) * math.exp(2 * lab - laa - lbb))
+
+    def versus_fp64(form: str) -> dict:
+        infid = []
+        for c in range(GRAD_VEC):  # final ansatz states, this form vs FP64
+            ab, lab = overlap(finals[form], c, finals["fp64"], c)
+            aa, laa = overlap(finals[form], c, finals[form], c)
+            bb, lbb = overlap(finals["fp64"], c, finals["fp64"], c)
+            infid.append(1.0 - abs(ab) ** 2 / (aa.real * bb.real) * math.exp(2 * lab - laa - lbb))
+        (e64, g64), (emx, gmx) = grads["fp64"], grads[form]
+        return {"max_abs_energy_diff": float(torch.max(torch.abs(emx - e64))),
+                "max_rel_grad_diff": float(torch.max(torch.abs(gmx - g64)) / torch.max(torch.abs(g64))),
+                "grad_rel_diff_median": float(torch.median(
+                    torch.amax(torch.abs(gmx - g64), dim=(1, 2, 3)) / torch.amax(torch.abs(g64), dim=(1, 2, 3)))),
+                "state_infidelity_median": float(np.median(infid)),
+                "state_infidelity_max": float(np.max(infid))}
+
+    cmp_mixed, cmp_all = versus_fp64("mixed"), versus_fp64("mixed_all")
     finals.clear()
-    (e64, g64), (emx, gmx) = grads["fp64"], grads["mixed"]
     res = {"workload": (f"{GRAD_VEC} parameter vectors of a {GRAD_N}-qubit hardware-efficient ansatz, "
                         f"{GRAD_LAYERS} layers (RY, RZ every site, CZ brick-wall), chi_max={GRAD_CHI}, "
                         f"transverse-field Ising energy J=h=1; energy + adjoint gradient per step; "
                         f"tapes kept in HBM (recompute false) or per-layer checkpoints + recomputation"),
-           "fp64": out["fp64"], "mixed": out["mixed"], "fp64_checkpointed": out["fp64_checkpointed"],
-           "mixed_form_note": ("at chi_cap <= 32 the mixed form runs the exact FP64 contraction (a 128-row "
-                               "tensor-core tile would be half padding) and differs from fp64 only by its "
-                               "Jacobi tolerance, 1e-9 against 1e-14"),
+           "fp64": out["fp64"], "mixed": out["mixed"], "mixed_all": out["mixed_all"],
+           "fp64_checkpointed": out["fp64_checkpointed"],
+           "mixed_form_note": ("at chi_cap <= 32 'mixed' runs the exact FP64 contraction and differs from fp64 only "
+                               "by its Jacobi tolerance, 1e-9 against 1e-14; 'mixed_all' takes the 3xTF32 "
+                               "tensor-core contraction here too (64-row tcgen05 tiles) with the 1e-6 S[0] floor"),
            "checkpointed_equals_taped": bool(torch.equal(grads["fp64"][1], grads["fp64_checkpointed"][1])),
-           "mixed_vs_fp64": {"max_abs_energy_diff": float(torch.max(torch.abs(emx - e64))),
-                             "max_rel_grad_diff": float(torch.max(torch.abs(gmx - g64)) / torch.max(torch.abs(g64))),
-                             "grad_rel_diff_median": float(torch.median(
-                                 torch.amax(torch.abs(gmx - g64), dim=(1, 2, 3)) / torch.amax(torch.abs(g64), dim=(1, 2, 3)))),
-                             "state_infidelity_median": float(np.median(infid)),
-                             "state_infidelity_max": float(np.max(infid)),
-                             "note": "per parameter vector; at chi_cap 32 the forms differ only by the Jacobi "
-                                     "tolerance (1e-9 vs 1e-14), the largest gradient differences on vectors "
-                                     "with near-degenerate singular values at the truncation boundary"},
+           "mixed_vs_fp64": dict(cmp_mixed, note=(
+               "per parameter vector; the largest gradient differences on vectors with near-degenerate singular "
+               "values at the truncation boundary")),
+           "mixed_all_vs_fp64": dict(cmp_all, note=(
+               "the tensor-core theta's ~1e-7 relative rounding and its 1e-6 S[0] floor change which values the "
+               "truncation keeps on these graded spectra")),
            "flops_per_step": flops}
     # adjoint vs parameter shift and central differences on the plain forward,
     # at this size (8 layers: bonds reach chi_max = 32 and truncate) and on a
@@ -295,10 +304,11 @@ def gradient_leg(dev, steps: int, warmup: int, rank: int, max_over_ranks, cpu_wo
     a0 = angles[0].cpu().numpy()
     check = gradient_check(dev, GRAD_N, GRAD_LAYERS, GRAD_CHI, a0,
                            {"fp64": grads["fp64"][1][0].cpu().numpy(),
-                            "mixed": grads["mixed"][1][0].cpu().numpy()}, SEED + 7)
+                            "mixed": grads["mixed"][1][0].cpu().numpy(),
+                            "mixed_all": grads["mixed_all"][1][0].cpu().numpy()}, SEED + 7)
     ctl_layers = 4
     ctl = {}
-    for prec in ("fp64", "mixed"):
+    for prec in ("fp64", "mixed", "mixed_all"):
         m4 = HEAEnergy(GRAD_N, ctl_layers, 1, chi_max=GRAD_CHI, cutoff=GRAD_CUT, precision=prec, device=dev)
         ctl[prec] = m4.energy_and_grad(a0[None, :ctl_layers])[1][0].cpu().numpy()
         del m4
@@ -712,23 +722,33 @@ def run_ours(args) -> None:
             b2.check_status()
         forms.clear()
 
-    # ---- per-update drop-in path (FP64, one update per call, no batching), one saturated layer
+    # ---- the drop-in called gate by gate, as mps_core users write it (FP64): the whole
+    # circuit as 990 MPSState._apply_adjacent_2q calls, then a read (flush), wall-clocked
+    # from the first call to the synchronised result; deferred (default) and eager
     single = None
     if not args.quick:
-        st1 = MPSState(N_SITES, CHI, CUTOFF, precision="fp64", device=dev)
-        st1._b.sites.copy_(batch.sites)
-        st1._b.bonds.copy_(batch.bonds)
-        L = layers[-1]
-        torch.cuda.synchronize()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record()
-        for i, g in zip(L.sites, L.gates):
-            st1._apply_adjacent_2q(int(i), g)
-        a1.record()
-        torch.cuda.synchronize()
-        single = {"updates_per_s": round(len(L.sites) / (a0.elapsed_time(a1) * 1e-3), 3),
-                  "note": "plain complex128 drop-in: MPSState._apply_adjacent_2q, one pair per launch, "
-                          "saturated chi=64 layer"}
+        calls = [(int(i), g) for L in layers for i, g in zip(L.sites, L.gates)]
+        runs = {}
+        for defer in (True, False):
+            for timed_run in (False, True):  # the first run sizes workspaces and kernel attributes
+                st1 = MPSState(N_SITES, CHI, CUTOFF, precision="fp64", device=dev, defer=defer)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                for i, g in calls:
+                    st1._apply_adjacent_2q(i, g)
+                st1.flush()
+                torch.cuda.synchronize()
+                wall = time.perf_counter() - t0
+            st1.check_status()
+            runs[defer] = (len(calls) / wall, st1)
+        same = all(torch.equal(x, y) for x, y in zip(runs[True][1]._b.snapshot(), runs[False][1]._b.snapshot()))
+        single = {"updates_per_s": round(runs[True][0], 3),
+                  "eager_updates_per_s": round(runs[False][0], 3),
+                  "bitwise_equal": bool(same),
+                  "note": ("plain complex128 drop-in called gate by gate (990 MPSState._apply_adjacent_2q calls of "
+                           "this circuit, then a read), wall clock: updates_per_s with the calls queued and run as one "
+                           "dataflow launch at the read (the default), eager_updates_per_s with one launch per call")}
+        del runs
 
     # ---- end to end through the public API, gates from pinned host memory, MPS read back
     e2e = None
@@ -776,7 +796,7 @@ def run_ours(args) -> None:
         cw = usable_cores() if (rank == 0 and world == 1 and not args.no_cpu) else 0
         torch.cuda.empty_cache()  # the 7.6 GB of tapes below should not fight the earlier legs' cached blocks
         gradient = gradient_leg(dev, 5, 3, rank, max_over_ranks, cpu_workers=cw)
-        for key in ("fp64", "mixed", "fp64_checkpointed"):  # fraction of the same FP64 roofline
+        for key in ("fp64", "mixed", "mixed_all", "fp64_checkpointed"):  # fraction of the same FP64 roofline
             gradient[key]["roofline_frac"] = round(gradient[key]["achieved_tflops"] / fp64_peak_tflops, 4)
 
     reps.close()
@@ -793,12 +813,15 @@ def run_ours(args) -> None:
                   "note": "batched per layer; mixed = 3xTF32 tcgen05 complex-3M theta + FP64 Jacobi SVD"},
         "target_ratio": {
             "batched_mixed_over_batched_fp64": round(mixed_v / fp64_v, 3),
-            "batched_mixed_over_per_update_fp64": (round(mixed_v / single["updates_per_s"], 2)
+            "batched_mixed_over_per_update_fp64": (round(mixed_v / single["eager_updates_per_s"], 2)
                                                    if single else None),
+            "batched_mixed_over_deferred_drop_in_fp64": (round(mixed_v / single["updates_per_s"], 2)
+                                                         if single else None),
             "target": ">= 5x the plain complex128 GPU form at infidelity <= 1e-6",
-            "note": ("first reading: both forms batched per layer (the mixed form moves only the ~5 % "
-                     "contraction share of an update onto the tensor cores; the FP64 Jacobi SVD is the rest); "
-                     "second reading: the plain form as the drop-in calls it, one update per launch")},
+            "note": ("first reading: both forms batched, one dataflow launch each (the mixed form moves only the "
+                     "~5 % contraction share of an update onto the tensor cores; the FP64 Jacobi SVD is the rest); "
+                     "second reading: the plain form as the drop-in runs it one update per launch; third: the "
+                     "drop-in called gate by gate with its calls queued into one dataflow launch")},
         "data": "synthetic (seeded Haar-random 4x4 gates, |0...0> start)",
         "config": {"workload": WORKLOAD, "precision": precision, "updates_per_step": n_upd,
                    "launches_per_step": 2, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",

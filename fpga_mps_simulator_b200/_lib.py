@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libmpsb200.so")
 MPSB_CHI_LIMIT = 64
 FP64 = 0
 MIXED_TF32X3 = 1
+TF32X3_ALL = 2
 ST_NOCONV, ST_NONFINITE, ST_BADDIM, ST_TIMEOUT, ST_CHI_LIMIT = 1, 2, 4, 8, 16
 
 

@@ -58,9 +58,11 @@ int check_device(const void *table, void *stream) {
 // The dynamic shared-memory limit is a per-device attribute of a kernel, so
 // the largest size enabled so far is remembered per (kernel, device), under a
 // lock (host threads may launch concurrently).  Called before each launch;
-// only a size above the remembered one reaches cudaFuncSetAttribute.
+// only a size above the remembered one reaches cudaFuncSetAttribute.  (Any
+// non-zero size is set: the default limit is 48 KB minus the kernel's static
+// shared memory, which several kernels here use.)
 int ensure_smem(const void *kernel, size_t bytes, const char *what) {
-    if (bytes <= 48 * 1024) return MPSB_OK;
+    if (bytes == 0) return MPSB_OK;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return set_error(MPSB_ENODEV, "no CUDA device");
     static std::mutex mu;
@@ -76,10 +78,8 @@ int ensure_smem(const void *kernel, size_t bytes, const char *what) {
 
 // kernels (update2q.cu, readout.cu)
 size_t upd_workspace_bytes(int npairs, int chi_cap);
-int launch_update2q(const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int, void *,
+int launch_update2q(int, const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int, void *,
                     double *, int32_t *, double *, int32_t *, cudaStream_t);
-int launch_update2q_mixed(const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int, void *,
-                          double *, int32_t *, double *, int32_t *, cudaStream_t);
 int launch_apply1q(const mpsb_chain *, const mpsb_site_op *, int, const double2 *, int, cudaStream_t);
 int launch_statevector(const mpsb_chain *, int, int, double2 *, double2 *, size_t, cudaStream_t);
 int launch_amplitude(const mpsb_chain *, int, int, const uint8_t *, int, double2 *, double *, cudaStream_t);
@@ -95,7 +95,7 @@ int launch_update2q_flow(const mpsb_chain *, int, const mpsb_flow_item *, int, c
                          const double2 *, int, int, double, int, int, int, int, void *, size_t, double *, int32_t *,
                          double *, int32_t *, cudaStream_t);
 size_t upd_tape_bytes(int npairs, int chi_cap);
-int launch_update2q_taped(bool, const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int,
+int launch_update2q_taped(int, const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int,
                           void *, void *, double *, int32_t *, double *, int32_t *, cudaStream_t);
 size_t bwd_workspace_bytes(int npairs, int chi_cap);
 int launch_update2q_backward(const mpsb_chain *, const mpsb_chain *, const mpsb_pair *, int, const double2 *, int,
@@ -144,7 +144,7 @@ int mpsb_update2q_batch(const mpsb_chain *chains, const mpsb_pair *pairs, int np
         return set_error(MPSB_EINVAL, "null chains/pairs/gates/status/workspace pointer");
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3)
+    if (!valid_precision(precision))
         return set_error(MPSB_EINVAL, "unknown precision %d", precision);
     const size_t need = upd_workspace_bytes(npairs, chi_cap);
     if (workspace_bytes < need)
@@ -154,28 +154,22 @@ int mpsb_update2q_batch(const mpsb_chain *chains, const mpsb_pair *pairs, int np
     int rc = check_device(chains, stream);
     if (rc) return rc;
     if (max_sweeps <= 0) max_sweeps = 40;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const double2 *g = reinterpret_cast<const double2 *>(gates);
-    if (precision == MPSB_FP64) {
-        if (tol <= 0.0) tol = 1.0e-14;
-        return launch_update2q(chains, pairs, npairs, g, chi_cap, tol, max_sweeps, workspace, spectra, kept, trunc,
-                               status, s);
-    }
-    if (tol <= 0.0) tol = 1.0e-9;
-    return launch_update2q_mixed(chains, pairs, npairs, g, chi_cap, tol, max_sweeps, workspace, spectra, kept,
-                                 trunc, status, s);
+    if (tol <= 0.0) tol = default_tol(precision);
+    return launch_update2q(precision, chains, pairs, npairs, reinterpret_cast<const double2 *>(gates), chi_cap, tol,
+                           max_sweeps, workspace, spectra, kept, trunc, status,
+                           reinterpret_cast<cudaStream_t>(stream));
 }
 
 size_t mpsb_update2q_flow_workspace_bytes(int nitems, int chi_cap, int precision, int threads, int nclusters) {
     if (nitems < 0 || chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT) return 0;
-    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3) return 0;
+    if (!valid_precision(precision)) return 0;
     return upd_flow_workspace_bytes(nitems, chi_cap, precision, threads, nclusters);
 }
 
 int mpsb_update2q_flow_clusters(int chi_cap, int precision, int threads) {
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3)
+    if (!valid_precision(precision))
         return set_error(MPSB_EINVAL, "unknown precision %d", precision);
     int rc = check_device(nullptr, nullptr);
     if (rc) return rc;
@@ -193,14 +187,14 @@ int mpsb_update2q_flow(const mpsb_chain *chains, int nchains, const mpsb_flow_it
         return set_error(MPSB_EINVAL, "null chains/items/chain_order/chain_offsets/gates/status/workspace pointer");
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3)
+    if (!valid_precision(precision))
         return set_error(MPSB_EINVAL, "unknown precision %d", precision);
     if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0)
         return set_error(MPSB_EINVAL, "workspace must be 256-byte aligned");
     int rc = check_device(chains, stream);
     if (rc) return rc;
     if (max_sweeps <= 0) max_sweeps = 40;
-    if (tol <= 0.0) tol = precision == MPSB_FP64 ? 1.0e-14 : 1.0e-9;
+    if (tol <= 0.0) tol = default_tol(precision);
     return launch_update2q_flow(chains, nchains, items, nitems, chain_order, chain_offsets,
                                 reinterpret_cast<const double2 *>(gates), precision, chi_cap, tol, max_sweeps,
                                 threads, nclusters, poll_limit, workspace, workspace_bytes, spectra, kept, trunc,
@@ -355,7 +349,7 @@ int mpsb_update2q_batch_taped(const mpsb_chain *chains, const mpsb_pair *pairs, 
         return set_error(MPSB_EINVAL, "null chains/pairs/gates/status/workspace/tape pointer");
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3)
+    if (!valid_precision(precision))
         return set_error(MPSB_EINVAL, "unknown precision %d", precision);
     const size_t need = upd_workspace_bytes(npairs, chi_cap);
     if (workspace_bytes < need)
@@ -367,9 +361,8 @@ int mpsb_update2q_batch_taped(const mpsb_chain *chains, const mpsb_pair *pairs, 
     int rc = check_device(chains, stream);
     if (rc) return rc;
     if (max_sweeps <= 0) max_sweeps = 40;
-    const bool mixed = precision == MPSB_MIXED_TF32X3;
-    if (tol <= 0.0) tol = mixed ? 1.0e-9 : 1.0e-14;
-    return launch_update2q_taped(mixed, chains, pairs, npairs, reinterpret_cast<const double2 *>(gates), chi_cap, tol,
+    if (tol <= 0.0) tol = default_tol(precision);
+    return launch_update2q_taped(precision, chains, pairs, npairs, reinterpret_cast<const double2 *>(gates), chi_cap, tol,
                                  max_sweeps, workspace, tape, spectra, kept, trunc, status,
                                  reinterpret_cast<cudaStream_t>(stream));
 }

@@ -41,9 +41,10 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo_bytes
            (static_cast<uint64_t>((sbo_bytes >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor: D f32, A and B tf32, both K-major, M = 128, N.
-__device__ __forceinline__ uint32_t make_idesc_tf32(int n) {
-    return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(n >> 3) << 17) | ((128u >> 4) << 24);
+// Instruction descriptor: D f32, A and B tf32, both K-major, M (64 or 128), N.
+__device__ __forceinline__ uint32_t make_idesc_tf32(int m, int n) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | (static_cast<uint32_t>(n >> 3) << 17) |
+           (static_cast<uint32_t>(m >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -119,14 +120,19 @@ __device__ __forceinline__ uint32_t core_off(int row, int k, int kc) {
 
 }  // namespace tc
 
-// Shapes of one CTA's GEMM.  Rows ("m", up to 128, padded to 128) run over the
-// index the CTA does not split, columns ("n", up to 64, padded to 16) over its
-// share of the split index, K over the shared bond chi_m (padded to 8):
+// Shapes of one CTA's GEMM.  Rows ("m", up to mt, padded to the MMA height
+// mt: 128 above chi_cap 32, 64 at or below it) run over the index the CTA
+// does not split, columns ("n", up to 64, padded to 16) over its share of the
+// split index, K over the shared bond chi_m (padded to 8):
 //   X = M   (no transpose): m = 2a + p (all a), n = 2(d - idx0) + q
 //   X = M^H (transpose):    m = 2d + q (all d), n = 2(a - idx0) + p
+// The accumulator of an M = 128 MMA holds row m in TMEM lane m; that of an
+// M = 64 MMA (one CTA) holds row m = m0 + 16 m1 (m0 < 16, m1 < 4) in lane
+// m0 + 32 m1, the first half of each warp's 32-lane quarter.
 struct TcShape {
-    int mvalid, nvalid, kpad, npad;
+    int mvalid, nvalid, kpad, npad, mt;
 };
+__device__ __forceinline__ int tmem_lane_of_row(int m, int mt) { return mt == 128 ? m : (m & 15) + 32 * (m >> 4); }
 
 // Operand value of the real product `prod` (0: Re, 1: Im, 2: Re + Im).
 __device__ __forceinline__ double part(double2 v, int prod) {
@@ -147,10 +153,11 @@ __device__ void stage_operands(unsigned char *buf, const double2 *A, const doubl
             return *q;
     };
     const int kc = sh.kpad >> 2;
-    const uint32_t abytes = 128u * sh.kpad * 4u, bbytes = static_cast<uint32_t>(sh.npad) * sh.kpad * 4u;
+    const uint32_t abytes = static_cast<uint32_t>(sh.mt) * sh.kpad * 4u;
+    const uint32_t bbytes = static_cast<uint32_t>(sh.npad) * sh.kpad * 4u;
     unsigned char *ahi = buf, *alo = buf + abytes, *bhi = buf + 2 * abytes, *blo = buf + 2 * abytes + bbytes;
-    // A operand: rows m < 128, one 16-byte chunk (4 k) per thread-iteration
-    const int achunks = 128 * kc;
+    // A operand: rows m < mt, one 16-byte chunk (4 k) per thread-iteration
+    const int achunks = sh.mt * kc;
     for (int e = tid; e < achunks; e += NT) {
         const int r8 = e & 7, c = (e >> 3) % kc, g = (e >> 3) / kc;
         const int m = g * 8 + r8, k0 = c * 4;
@@ -200,10 +207,11 @@ __device__ void stage_operands(unsigned char *buf, const double2 *A, const doubl
 // One thread issues the 3xTF32 MMAs of a product into accumulator column `dcol`.
 __device__ __forceinline__ void issue_product(unsigned char *buf, uint32_t tmem, int dcol, const TcShape &sh) {
     const int kc = sh.kpad >> 2;
-    const uint32_t abytes = 128u * sh.kpad * 4u, bbytes = static_cast<uint32_t>(sh.npad) * sh.kpad * 4u;
+    const uint32_t abytes = static_cast<uint32_t>(sh.mt) * sh.kpad * 4u;
+    const uint32_t bbytes = static_cast<uint32_t>(sh.npad) * sh.kpad * 4u;
     const uint32_t ahi = tc::smem_u32(buf), alo = ahi + abytes, bhi = ahi + 2 * abytes, blo = bhi + bbytes;
     const uint32_t sbo = static_cast<uint32_t>(kc) * 128u;
-    const uint32_t idesc = tc::make_idesc_tf32(sh.npad);
+    const uint32_t idesc = tc::make_idesc_tf32(sh.mt, sh.npad);
     const uint32_t d = tmem + static_cast<uint32_t>(dcol);
     for (int s = 0; s < (sh.kpad >> 3); ++s) {
         const uint32_t step = static_cast<uint32_t>(s) * 256u;  // two 16-byte K chunks per K = 8 step
@@ -216,18 +224,22 @@ __device__ __forceinline__ void issue_product(unsigned char *buf, uint32_t tmem,
 // Read the three accumulators back, form T = P1 - P2 + i (P3 - P1 - P2),
 // apply the gate in FP64 and write theta into the Jacobi slots (X) and the
 // workspace copy (x0), in the same positions the FP64 path uses.  Warp w
-// reads TMEM lanes 32 (w & 3) .. +31 (= rows m) and 16-column chunks w >> 2,
-// w >> 2 + 2, ...; the two values of a row pair (m, m ^ 1) meet by shuffle.
+// reads TMEM lanes 32 (w & 3) .. +31 and 16-column chunks w >> 2,
+// w >> 2 + NT / 128, ...; its lanes hold rows m = 32 (w & 3) + lane (M = 128)
+// or, in lanes 0..15, rows m = 16 (w & 3) + lane (M = 64).  The two values of
+// a row pair (m, m ^ 1) meet by shuffle.  Rows no warp reads (M = 64 with two
+// warps: rows 32..63) must be padding (mvalid <= 32).
 template <int NT>
 __device__ void read_theta(uint32_t tmem, const TcShape &sh, const double2 *g, bool trans, int cr, int C,
                            int idx0, int nidx, int w, int wmax, int rpad, double2 *X, double2 *x0, int tid,
                            int &nonfin) {
     const int warp = tid >> 5, lane = tid & 31;
     const int qr = warp & 3;
-    const int m = 32 * qr + lane;
-    const bool mval = m < sh.mvalid;
+    const int m = sh.mt == 128 ? 32 * qr + lane : 16 * qr + lane;
+    const bool mval = m < sh.mvalid && (sh.mt == 128 || lane < 16);
     const int nchunks = sh.npad >> 4;
-    for (int ch = warp >> 2; ch < nchunks; ch += NT / 128) {
+    constexpr int kChunkStride = NT >= 256 ? NT / 128 : 1;
+    for (int ch = warp >> 2; ch < nchunks; ch += kChunkStride) {
         const uint32_t base = tmem + (static_cast<uint32_t>(32 * qr) << 16) + static_cast<uint32_t>(16 * ch);
         float p1[16], p2[16], p3[16];
         tc::tmem_ld16(base, p1);
@@ -300,6 +312,7 @@ __device__ bool contract_mixed(unsigned char *opbuf, uint64_t *mbar, uint32_t *t
     sh.nvalid = 2 * nidx;
     sh.npad = max(16, (sh.nvalid + 15) & ~15);
     sh.kpad = (cm + 7) & ~7;
+    sh.mt = rpad > 64 ? 128 : 64;  // rows of a column: 128 above chi_cap 32, at most 64 below
     const int need = 3 * sh.npad;
     const uint32_t ncols = need <= 32 ? 32u : need <= 64 ? 64u : need <= 128 ? 128u : 256u;
     if ((tid >> 5) == 0) tc::tmem_alloc(tmem_slot, ncols);

@@ -63,6 +63,13 @@ __host__ __device__ inline int keep_limit(const mpsb_chain &ch) {
     return k < schmidt ? k : schmidt;
 }
 
+__host__ __device__ inline bool valid_precision(int p) {
+    return p == MPSB_FP64 || p == MPSB_MIXED_TF32X3 || p == MPSB_TF32X3_ALL;
+}
+// Jacobi off-diagonal tolerance of a form when the caller passes none: the
+// tensor-core forms' theta carries ~1e-7 relative rounding, so they stop at 1e-9.
+__host__ __device__ inline double default_tol(int p) { return p == MPSB_FP64 ? 1.0e-14 : 1.0e-9; }
+
 // Per-pair bookkeeping written by the update kernel, folded into norm_log by
 // a second kernel in pair order.
 struct PairRec {

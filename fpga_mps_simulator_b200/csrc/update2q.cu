@@ -103,12 +103,14 @@ __host__ __device__ inline size_t upd_smem_bytes(int wmax, int rpad) {
     return upd_qr_offset(wmax, rpad) + sizeof(QrScratch);
 }
 // The mixed form stages tensor-core operands from the slot area onwards
-// (hi and lo tf32 of a 128 x kpad A operand and an npad x kpad B operand);
-// everything it overlaps is written only after the contraction.
+// (hi and lo tf32 of an mt x kpad A operand -- mt = 128 rows above chi_cap
+// 32, 64 below -- and an npad x kpad B operand); everything it overlaps is
+// written only after the contraction.
 __host__ __device__ inline size_t upd_smem_bytes_mixed(int wmax, int rpad, int chi_cap) {
     const size_t kpad = (size_t)((chi_cap + 7) & ~7);
     const size_t npad = (size_t)(((2 * wmax) + 15) & ~15) < 16 ? 16 : (size_t)(((2 * wmax) + 15) & ~15);
-    const size_t ops = 2 * 128 * kpad * 4 + 2 * npad * kpad * 4;
+    const size_t mt = rpad > 64 ? 128 : 64;
+    const size_t ops = 2 * mt * kpad * 4 + 2 * npad * kpad * 4;
     const size_t base = upd_smem_bytes(wmax, rpad);
     return (384 + ops > base) ? 384 + ops : base;
 }
@@ -1570,7 +1572,7 @@ static int launch_rpl(const Upd2Params &p, size_t smem, cudaStream_t s) {
     return check_launch("update2q kernel");
 }
 
-static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+static int launch_update2q_impl(int precision, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
                                 const double2 *gates, int chi_cap, double tol, int max_sweeps, void *ws,
                                 double *spectra, int32_t *kept, double *trunc, int32_t *status, cudaStream_t stream,
                                 void *tape = nullptr) {
@@ -1603,12 +1605,14 @@ static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb
     p.wmax = (((2 * chi_cap) + 15) & ~15) / 4;
     p.tol2 = tol * tol;
     p.max_sweeps = max_sweeps;
-    // At chi_cap <= 32 a 128-row tensor-core tile is half padding or more and
-    // the FP64 contraction is both exact and faster (measured per 64-vector
-    // ansatz forward: 37 vs 55 ms at chi = 16, 96.9 vs 104.9 ms at chi = 32),
-    // so the mixed form uses it there (and keeps only its looser Jacobi
-    // tolerance).
-    if (mixed && rpl <= 2) mixed = false;
+    // MPSB_MIXED_TF32X3: at chi_cap <= 32 the FP64 contraction is exact and
+    // was faster than a 128-row tensor-core tile (half padding or more;
+    // measured per 64-vector ansatz forward: 37 vs 55 ms at chi = 16, 96.9 vs
+    // 104.9 ms at chi = 32), so that form keeps it there (and only its looser
+    // Jacobi tolerance).  MPSB_TF32X3_ALL takes the tensor cores at every cap,
+    // with a 64-row tile at chi_cap <= 32.
+    bool mixed = precision != MPSB_FP64;
+    if (precision == MPSB_MIXED_TF32X3 && rpl <= 2) mixed = false;
     // 3xTF32 theta carries relative errors near 1e-7, so singular values below
     // ~1e-6 S[0] are rounding noise: the mixed form never keeps them
     p.cut_floor = mixed ? kMixedCutoffFloor : 0.0;
@@ -1617,11 +1621,15 @@ static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb
     // CTA size follows the column count: a slot of C/4 columns holds C/16
     // quads and a round has at most that many quad tasks per slot pair, so
     // 128 threads (64 at chi_cap <= 16) keep every warp busy and let two or
-    // more clusters share an SM pair; the tensor-core readout of the mixed
-    // form (chi_cap > 32 only) needs whole 128-thread groups (one warp per
-    // TMEM lane quarter).
-    if (mixed) {  // rpl == 4 here: smaller caps run the FP64 contraction (above)
-        rc = launch_rpl<4, kUpdThreads, true>(p, smem, stream);
+    // more clusters share an SM pair; the tensor-core read-out takes one warp
+    // per TMEM lane quarter that holds rows (four at chi_cap > 16, two below).
+    if (mixed) {
+        if (rpl == 1)
+            rc = launch_rpl<1, 64, true>(p, smem, stream);
+        else if (rpl == 2)
+            rc = launch_rpl<2, 128, true>(p, smem, stream);
+        else
+            rc = launch_rpl<4, kUpdThreads, true>(p, smem, stream);
     } else {
         if (rpl == 1)
             rc = launch_rpl<1, 64, false>(p, smem, stream);
@@ -1635,17 +1643,10 @@ static int launch_update2q_impl(bool mixed, const mpsb_chain *chains, const mpsb
     return check_launch("fold_norm_log_kernel");
 }
 
-int launch_update2q(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const double2 *gates,
-                    int chi_cap, double tol, int max_sweeps, void *ws, double *spectra, int32_t *kept,
-                    double *trunc, int32_t *status, cudaStream_t stream) {
-    return launch_update2q_impl(false, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
-                                trunc, status, stream);
-}
-
-int launch_update2q_mixed(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const double2 *gates,
-                          int chi_cap, double tol, int max_sweeps, void *ws, double *spectra, int32_t *kept,
-                          double *trunc, int32_t *status, cudaStream_t stream) {
-    return launch_update2q_impl(true, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
+int launch_update2q(int precision, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+                    const double2 *gates, int chi_cap, double tol, int max_sweeps, void *ws, double *spectra,
+                    int32_t *kept, double *trunc, int32_t *status, cudaStream_t stream) {
+    return launch_update2q_impl(precision, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
                                 trunc, status, stream);
 }
 
@@ -1668,14 +1669,20 @@ int flow_shape(int chi_cap, int precision, int threads, FlowShape &sh) {
     const bool ok = (sh.rpl == 1 && (sh.nt == 64 || sh.nt == 128)) || (sh.rpl == 2 && (sh.nt == 128 || sh.nt == 256)) ||
                     (sh.rpl == 4 && sh.nt == 256);
     if (!ok) return set_error(MPSB_EINVAL, "threads=%d is not a CTA shape for chi_cap=%d", threads, chi_cap);
-    sh.mixed = precision == MPSB_MIXED_TF32X3 && sh.rpl == 4;
+    sh.mixed = (precision == MPSB_MIXED_TF32X3 && sh.rpl == 4) || precision == MPSB_TF32X3_ALL;
+    if (sh.mixed && sh.nt != deflt)  // the tensor-core forms are built for the default CTA sizes only
+        return set_error(MPSB_EINVAL, "threads=%d: the tensor-core form at chi_cap=%d runs %d threads", threads,
+                         chi_cap, deflt);
     const int wmax = (((2 * chi_cap) + 15) & ~15) / 4, rpad = 32 * sh.rpl;
     sh.smem = sh.mixed ? upd_smem_bytes_mixed(wmax, rpad, chi_cap) : upd_smem_bytes(wmax, rpad);
     return MPSB_OK;
 }
 
 const void *flow_kernel_ptr(const FlowShape &sh) {
-    if (sh.mixed) return reinterpret_cast<const void *>(update2q_flow_kernel<4, kUpdThreads, true>);
+    if (sh.mixed)
+        return sh.rpl == 1   ? reinterpret_cast<const void *>(update2q_flow_kernel<1, 64, true>)
+               : sh.rpl == 2 ? reinterpret_cast<const void *>(update2q_flow_kernel<2, 128, true>)
+                             : reinterpret_cast<const void *>(update2q_flow_kernel<4, kUpdThreads, true>);
     if (sh.rpl == 1)
         return sh.nt == 64 ? reinterpret_cast<const void *>(update2q_flow_kernel<1, 64, false>)
                            : reinterpret_cast<const void *>(update2q_flow_kernel<1, 128, false>);
@@ -1799,7 +1806,9 @@ int launch_update2q_flow(const mpsb_chain *chains, int nchains, const mpsb_flow_
     p.cut_floor = sh.mixed ? kMixedCutoffFloor : 0.0;
     if (cudaMemsetAsync(w, 0, flags, stream) != cudaSuccess) return check_launch("cudaMemsetAsync(flow flags)");
     if (sh.mixed)
-        rc = launch_flow_rpl<4, kUpdThreads, true>(p, f, sh.smem, stream);
+        rc = sh.rpl == 1   ? launch_flow_rpl<1, 64, true>(p, f, sh.smem, stream)
+             : sh.rpl == 2 ? launch_flow_rpl<2, 128, true>(p, f, sh.smem, stream)
+                           : launch_flow_rpl<4, kUpdThreads, true>(p, f, sh.smem, stream);
     else if (sh.rpl == 1)
         rc = sh.nt == 64 ? launch_flow_rpl<1, 64, false>(p, f, sh.smem, stream)
                          : launch_flow_rpl<1, 128, false>(p, f, sh.smem, stream);
@@ -1813,10 +1822,10 @@ int launch_update2q_flow(const mpsb_chain *chains, int nchains, const mpsb_flow_
     return check_launch("fold_flow_kernel");
 }
 
-int launch_update2q_taped(bool mixed, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+int launch_update2q_taped(int precision, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
                           const double2 *gates, int chi_cap, double tol, int max_sweeps, void *ws, void *tape,
                           double *spectra, int32_t *kept, double *trunc, int32_t *status, cudaStream_t stream) {
-    return launch_update2q_impl(mixed, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
+    return launch_update2q_impl(precision, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
                                 trunc, status, stream, tape);
 }
 

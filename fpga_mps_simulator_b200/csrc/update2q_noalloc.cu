@@ -31,10 +31,8 @@
 namespace mpsb {
 
 size_t upd_workspace_bytes(int npairs, int chi_cap);
-int launch_update2q(const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int, void *,
+int launch_update2q(int, const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int, void *,
                     double *, int32_t *, double *, int32_t *, cudaStream_t);
-int launch_update2q_mixed(const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double, int, void *,
-                          double *, int32_t *, double *, int32_t *, cudaStream_t);
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[MPSB_NOALLOC_SCRATCH_BYTES];
 
@@ -77,8 +75,7 @@ extern "C" int mpsb_update2q_batch_noalloc(const mpsb_chain *chains, const mpsb_
         return set_error(MPSB_EINVAL, "null chains/pairs/gates/status pointer");
     if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
         return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
-    if (precision != MPSB_FP64 && precision != MPSB_MIXED_TF32X3)
-        return set_error(MPSB_EINVAL, "unknown precision %d", precision);
+    if (!valid_precision(precision)) return set_error(MPSB_EINVAL, "unknown precision %d", precision);
     const size_t need = upd_workspace_bytes(npairs, chi_cap);
     if (need > (size_t)MPSB_NOALLOC_SCRATCH_BYTES)
         return set_error(MPSB_EWORKSPACE,
@@ -91,14 +88,7 @@ extern "C" int mpsb_update2q_batch_noalloc(const mpsb_chain *chains, const mpsb_
     rc = noalloc_scratch(&scratch);
     if (rc) return rc;
     if (max_sweeps <= 0) max_sweeps = 40;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    const double2 *g = reinterpret_cast<const double2 *>(gates);
-    if (precision == MPSB_FP64) {
-        if (tol <= 0.0) tol = 1.0e-14;
-        return launch_update2q(chains, pairs, npairs, g, chi_cap, tol, max_sweeps, scratch, spectra, kept, trunc,
-                               status, s);
-    }
-    if (tol <= 0.0) tol = 1.0e-9;
-    return launch_update2q_mixed(chains, pairs, npairs, g, chi_cap, tol, max_sweeps, scratch, spectra, kept, trunc,
-                                 status, s);
+    if (tol <= 0.0) tol = default_tol(precision);
+    return launch_update2q(precision, chains, pairs, npairs, reinterpret_cast<const double2 *>(gates), chi_cap, tol,
+                           max_sweeps, scratch, spectra, kept, trunc, status, reinterpret_cast<cudaStream_t>(stream));
 }

@@ -34,8 +34,11 @@ from .gates import GATE_MATRICES, permute_2q
 __all__ = ["MPSState", "MPSBatch", "PairBatch", "FlowBatch", "PRECISIONS", "validate_pairs", "flow_items", "overlap",
            "infidelity"]
 
+# "mixed": 3xTF32 tensor-core theta where it fills a 128-row tile (chi_cap > 32),
+# the exact FP64 contraction below; "mixed_all": the tensor cores at every cap
+# (64-row tiles at chi_cap <= 32).  Both: FP64 Jacobi SVD, 1e-6 S[0] floor.
 PRECISIONS = {"fp64": _lib.FP64, "complex128": _lib.FP64, "mixed": _lib.MIXED_TF32X3,
-              "tf32x3": _lib.MIXED_TF32X3}
+              "tf32x3": _lib.MIXED_TF32X3, "mixed_all": _lib.TF32X3_ALL}
 _SWAP = GATE_MATRICES["swap"]
 
 
@@ -603,21 +606,61 @@ class MPSState:
     read-out then raises instead of returning a state that differs from the
     reference's.  ``precision`` selects the FP64 drop-in form or the mixed
     3xTF32 form.
+
+    Gate-by-gate use, as mps_core callers write it: ``_apply_adjacent_2q`` /
+    ``apply_2q`` calls are queued (``defer=True``, the default) and run as
+    ONE dataflow launch when the state is next read or changed in another
+    way, or when ``flush_at`` updates are waiting: each update starts as soon
+    as the earlier updates on its two sites are done, so disjoint gates of a
+    circuit run side by side instead of one 2-CTA cluster at a time.  The
+    result is bit-identical to applying them one by one (``defer=False``).
+    Argument errors still raise at the call.
     """
 
     def __init__(self, n: int, chi_max: int = 256, svd_cutoff: float = 1e-12, precision: str = "fp64",
-                 device: Union[str, torch.device] = "cuda", tol: float = 0.0, max_sweeps: int = 0):
+                 device: Union[str, torch.device] = "cuda", tol: float = 0.0, max_sweeps: int = 0,
+                 defer: bool = True, flush_at: int = 4096):
         self.n = int(n)
         self.chi_max = int(chi_max)
         self.svd_cutoff = float(svd_cutoff)
-        self._b = MPSBatch([self.n], [self.chi_max], [self.svd_cutoff], precision, device, tol, max_sweeps)
+        self._batch = MPSBatch([self.n], [self.chi_max], [self.svd_cutoff], precision, device, tol, max_sweeps)
         self.precision = precision
-        self._one = {}
-        self.last_pairs: Optional[PairBatch] = None
+        self.defer = bool(defer)
+        self.flush_at = int(flush_at)
+        self._pending: List[Tuple[int, np.ndarray]] = []
+        self._last_pairs: Optional[PairBatch] = None
+        self.last_flow: Optional[FlowBatch] = None
+
+    @property
+    def _b(self) -> MPSBatch:
+        """The device batch, with every queued update applied first."""
+        if self._pending:
+            self.flush()
+        return self._batch
+
+    def flush(self) -> None:
+        """Launch the queued two-site updates (one dataflow launch; asynchronous)."""
+        if not self._pending:
+            return
+        sites = np.array([p[0] for p in self._pending], np.int32)
+        gates = np.stack([p[1] for p in self._pending])
+        self._pending = []
+        self.last_flow = self._batch.make_flow(np.zeros(len(sites), np.int32), sites, gates)
+        self._batch.run_flow(self.last_flow)
+
+    @property
+    def last_pairs(self) -> Optional[PairBatch]:
+        """Per-update outputs of the last ``apply_layer`` (or undeferred update)."""
+        self.flush()
+        return self._last_pairs
+
+    @last_pairs.setter
+    def last_pairs(self, pb: Optional[PairBatch]) -> None:
+        self._last_pairs = pb
 
     @property
     def device(self) -> torch.device:
-        return self._b.device
+        return self._batch.device
 
     # -- state -------------------------------------------------------------
     @property
@@ -642,7 +685,7 @@ class MPSState:
 
     def copy(self) -> "MPSState":
         out = MPSState(self.n, self.chi_max, self.svd_cutoff, self.precision, self.device,
-                       self._b.tol, self._b.max_sweeps)
+                       self._b.tol, self._b.max_sweeps, self.defer, self.flush_at)
         out._b.sites.copy_(self._b.sites)
         out._b.bonds.copy_(self._b.bonds)
         out._b.norm_logs.copy_(self._b.norm_logs)
@@ -670,8 +713,20 @@ class MPSState:
         self._b.apply_1q_many([0], [int(site)], np.asarray(gate, np.complex128).reshape(1, 2, 2))
 
     def _apply_adjacent_2q(self, i: int, gate: np.ndarray) -> None:
-        """contract -> gate -> truncated SVD -> sqrt(S) split on (i, i+1) (mps_core.py:326-350)."""
-        self.last_pairs = self._b.apply_layer([0], [int(i)], np.asarray(gate, np.complex128).reshape(1, 4, 4))
+        """contract -> gate -> truncated SVD -> sqrt(S) split on (i, i+1) (mps_core.py:326-350).
+
+        Queued when ``defer`` is set (see the class notes); the gate is copied
+        at the call."""
+        i = int(i)
+        if not 0 <= i < self.n - 1:
+            raise ValueError(f"pair site out of range: need 0 <= i and i + 1 < n, got i={i}, n={self.n}")
+        g = np.array(gate, dtype=np.complex128).reshape(4, 4)
+        if not self.defer:
+            self.last_pairs = self._b.apply_layer([0], [i], g[None])
+            return
+        self._pending.append((i, g))
+        if len(self._pending) >= self.flush_at:
+            self.flush()
 
     apply_adjacent_2q = _apply_adjacent_2q
 

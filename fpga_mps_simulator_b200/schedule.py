@@ -301,6 +301,8 @@ def autotune(schedule: Schedule, start: int = 0, layers: int = 4, repeats: int =
     rflow = Runner(schedule, "flow")
     for cap in schedule.caps():
         menu = _lib.FLOW_THREADS[_lib.rows_per_lane(cap)]
+        if b.precision == "mixed_all" or (b.precision in ("mixed", "tf32x3") and _lib.rows_per_lane(cap) == 4):
+            menu = menu[:1]  # the tensor-core forms are built for the default CTA size only
         ms = {nt: best_of(lambda: rflow._run_flow(start, hi, only_cap=cap, threads=nt)) for nt in menu}
         shapes[cap] = min(ms, key=ms.get)
         shape_ms[f"chi{cap}"] = {nt: round(v, 3) for nt, v in ms.items()}

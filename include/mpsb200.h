@@ -97,7 +97,11 @@ enum mpsb_precision {
                              the contraction runs in FP64 (exact, no floor): the 128-row
                              tensor-core tile would be half padding or more, and the form
                              then differs from MPSB_FP64 only by its Jacobi tolerance
-                             (1e-9 against 1e-14)                                        */
+                             (1e-9 against 1e-14)                                        */,
+    MPSB_TF32X3_ALL = 2   /* the 3xTF32 tensor-core theta at EVERY bond cap (M = 64 MMA
+                             tiles at chi_cap <= 32, M = 128 above), FP64 Jacobi SVD, the
+                             same 1e-6 S[0] floor and 1e-9 Jacobi tolerance as
+                             MPSB_MIXED_TF32X3                                           */
 };
 
 enum mpsb_status_bits {

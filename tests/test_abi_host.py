@@ -74,6 +74,36 @@ def test_keep_limit_and_status_names():
     assert re.search(r"MPSB_ST_CHI_LIMIT\s*=\s*16", hdr) and re.search(r"MPSB_ST_TIMEOUT\s*=\s*8", hdr)
 
 
+def test_library_calls_run_with_the_owner_device_current(monkeypatch):
+    # every entry point launches on the current device, so a batch on cuda:1
+    # must make cuda:1 current around each call, whatever the caller has current
+    import torch
+    seen = []
+
+    class Ctx:
+        def __init__(self, d):
+            self.d = d
+
+        def __enter__(self):
+            seen.append(("enter", self.d))
+
+        def __exit__(self, *exc):
+            seen.append(("exit", self.d))
+
+    class FakeLib:
+        version = "not a call"
+
+        def mpsb_probe(self, x):
+            seen.append(("call", x))
+            return 7
+
+    monkeypatch.setattr(torch.cuda, "device", Ctx)
+    lib = _lib.OnDevice(FakeLib(), "cuda:1")
+    assert lib.mpsb_probe(3) == 7
+    assert seen == [("enter", "cuda:1"), ("call", 3), ("exit", "cuda:1")]
+    assert lib.version == "not a call"
+
+
 def test_validate_pairs():
     validate_pairs([10], [0, 0, 0], [0, 2, 8])
     validate_pairs([10, 6], [0, 0, 1, 1], [1, 5, 0, 4])

@@ -90,6 +90,45 @@ def test_entropy_and_bond_spectrum_follow_reference_gauge(key, chi, cut):
     assert abs(m.entanglement_entropy(b) - st.exact_entanglement_entropy(b)) < 1e-9
 
 
+def test_deferred_gate_by_gate_calls_equal_eager_calls_bitwise():
+    """The drop-in queues _apply_adjacent_2q / apply_2q calls and runs them as one
+    dataflow launch at the next read; the state must be exactly what one launch per
+    call gives -- with SWAP routing, reversed pairs and single-site gates in between
+    (each of which flushes the queue first)."""
+    from fpga_mps_simulator_b200 import MPSState, gate_1q
+    from fpga_mps_simulator_b200.circuits import haar_4x4
+    rng = np.random.default_rng(17)
+    n = 10
+    ops = []
+    for _ in range(60):
+        r = rng.random()
+        if r < 0.7:
+            i = int(rng.integers(0, n - 1))
+            ops.append(("2", i, i + 1, haar_4x4(rng)))
+        elif r < 0.8:
+            i, j = (int(v) for v in rng.choice(n, 2, replace=False))
+            ops.append(("2", i, j, haar_4x4(rng)))  # routed or reversed
+        else:
+            ops.append(("1", int(rng.integers(0, n)), gate_1q("u", list(rng.uniform(-3, 3, 3)))))
+    ops.append(("2", 3, 4, haar_4x4(rng)))  # end on a two-site gate: it stays queued until the read
+    states = {}
+    for defer in (True, False):
+        st = MPSState(n, 16, 1e-12, defer=defer)
+        for op in ops:
+            if op[0] == "2":
+                st.apply_2q(op[1], op[2], op[3])
+            else:
+                st.apply_1q(op[1], op[2])
+        states[defer] = st
+    d, e = states[True], states[False]
+    assert len(d._pending) > 0  # the last calls are still queued; reading _b below flushes them
+    for x, y in zip(d._b.snapshot(), e._b.snapshot()):
+        assert torch.equal(x, y)
+    assert d.last_flow is not None and d.norm_log == e.norm_log
+    with pytest.raises(ValueError, match="range"):
+        d._apply_adjacent_2q(n - 1, np.eye(4))
+
+
 def test_chain_table_in_host_memory_is_refused():
     from fpga_mps_simulator_b200 import MPSBatch, _lib
     b = MPSBatch([4], 4, 1e-12)

@@ -22,12 +22,14 @@ def _sites(st):
     return [st.sites[k] for k in range(st.n)]
 
 
+@pytest.mark.parametrize("precision", ["mixed", "mixed_all"])
 @pytest.mark.parametrize("name", ["brick_n16_d10_chi16", "brick_n40_d16_chi32", "brick_n20_d12_chi64"])
-def test_mixed_spectra_and_fidelity_on_golden(name):
+def test_mixed_spectra_and_fidelity_on_golden(name, precision):
+    """"mixed_all" runs the tensor cores at chi_cap 16 and 32 too (64-row MMA tiles)."""
     from fpga_mps_simulator_b200 import MPSState
     g = load_golden(name)
     n = int(g["n"])
-    st = MPSState(n, int(g["chi_max"]), float(g["cutoff"]), precision="mixed")
+    st = MPSState(n, int(g["chi_max"]), float(g["cutoff"]), precision=precision)
     ref = OracleMPS(n, int(g["chi_max"]), float(g["cutoff"]))
     k0 = 0
     layer_sites, layer_gates = [], []
@@ -51,6 +53,32 @@ def test_mixed_spectra_and_fidelity_on_golden(name):
         k0 += len(sites)
     st.check_status()
     assert infidelity(_sites(st), ref.sites) <= INFID
+
+
+@pytest.mark.parametrize("chi", [8, 16, 32])
+def test_mixed_all_runs_the_tensor_cores_below_chi_64(chi):
+    """At chi_cap <= 32 "mixed" keeps the exact FP64 contraction (spectra equal to
+    FP64 up to the Jacobi tolerance) while "mixed_all" takes the 64-row
+    tensor-core tile: its theta rounding (~1e-7 relative) shows in the spectra,
+    within the mixed form's 1e-5 S[0] budget."""
+    from fpga_mps_simulator_b200 import MPSState
+    n, depth = 12, 6
+    layers = brickwall_layers(n, depth, 77 + chi)
+    out = {}
+    for prec in ("fp64", "mixed_all"):
+        st = MPSState(n, chi, 1e-12, precision=prec)
+        spec = [st.apply_layer(L.sites, L.gates, record_spectra=True).spectra.cpu().numpy() for L in layers]
+        st.check_status()
+        out[prec] = (np.concatenate(spec), st)
+    a, b = out["fp64"][0], out["mixed_all"][0]
+    s0 = np.max(a, axis=1, keepdims=True)
+    diff = np.max(np.abs(a - b) / s0)
+    assert 1e-12 < diff < SV_TOL, diff
+    ref = OracleMPS(n, chi, 1e-12)
+    for L in layers:
+        for i, g in zip(L.sites, L.gates):
+            ref.apply_adjacent_2q(int(i), g)
+    assert infidelity(_sites(out["mixed_all"][1]), ref.sites) <= INFID
 
 
 def test_mixed_precision_config_against_fp64():
