@@ -242,35 +242,79 @@ __device__ void trace_normalise(double2 *E, int dim, double *red, int tid, int n
     __syncthreads();
 }
 
-// One CTA per chain: left environments envL[k] (k = 0..n) and right
+// Two CTAs per chain, one per direction: left environments envL[k] (k = 0..n) and right
 // environments envR[k], chi_cap x chi_cap each, trace-normalised per site.
+// The environment sweeps' steps as two CTA GEMMs each on the FP64
+// tensor-core MMA (the whole 256-thread CTA; T in global scratch):
+//   left:  T[x, (t,d)] = sum_y E[x,y] A[y,(t,d)];  E'[c,d] = sum_(x,s) conj(A[(x,s),c]) T[(x,s),d]
+//   right: T[(d,s), x] = sum_y A[(d,s),y] F[x,y];  F'[c,d] = sum_(s,x) conj(A[c,(s,x)]) T[d,(s,x)]
+// (the loops of left_step / right_step for the plain environments, 7-8x
+// fewer cycles per step at chi = 64).
+__device__ void left_env_step_mma(const double2 *E, const EnvStepArgs &a, double2 *T, double2 *Eout,
+                                  GemmSmem &sm) {
+    const int cl = a.cl, cr = a.cr, twocr = 2 * cr;
+    cta_cgemm<true, true>(
+        cl, twocr, cl, [&](int x, int y) { return E[x * cl + y]; },
+        [&](int y, int j) { return a.A[(size_t)y * twocr + j]; },
+        [&](int x, int j, double2 v) { T[(size_t)x * twocr + j] = v; }, sm);
+    __threadfence_block();
+    __syncthreads();
+    cta_cgemm<false, true>(
+        cr, cr, 2 * cl, [&](int c, int k) { return c_conj(a.A[(size_t)k * cr + c]); },
+        [&](int k, int d) { return T[(size_t)k * cr + d]; }, [&](int c, int d, double2 v) { Eout[c * cr + d] = v; },
+        sm);
+    __syncthreads();
+}
+
+__device__ void right_env_step_mma(const double2 *F, const EnvStepArgs &a, double2 *T, double2 *Fout,
+                                   GemmSmem &sm) {
+    const int cl = a.cl, cr = a.cr, twocr = 2 * cr;
+    cta_cgemm<true, false>(
+        2 * cl, cr, cr, [&](int i, int y) { return a.A[(size_t)i * cr + y]; },
+        [&](int y, int x) { return F[x * cr + y]; }, [&](int i, int x, double2 v) { T[(size_t)i * cr + x] = v; },
+        sm);
+    __threadfence_block();
+    __syncthreads();
+    cta_cgemm<true, false>(
+        cl, cl, twocr, [&](int c, int k) { return c_conj(a.A[(size_t)c * twocr + k]); },
+        [&](int k, int d) { return T[(size_t)d * twocr + k]; }, [&](int c, int d, double2 v) { Fout[c * cl + d] = v; },
+        sm);
+    __syncthreads();
+}
+
 __global__ void environments_kernel(const mpsb_chain *chains, int n, int chi_cap, double2 *envL, double2 *envR,
                                     double2 *tscr) {
+    __shared__ GemmSmem gsm;
     extern __shared__ __align__(16) unsigned char sm[];
     double2 *E = reinterpret_cast<double2 *>(sm);
     double2 *En = E + chi_cap * chi_cap;
     __shared__ double red[32];
     const int tid = threadIdx.x, nth = blockDim.x;
-    const mpsb_chain ch = chains[blockIdx.x];
+    const int chain = blockIdx.x >> 1;
+    const bool left = (blockIdx.x & 1) == 0;  // CTA 2c sweeps left to right, CTA 2c + 1 right to left
+    const mpsb_chain ch = chains[chain];
     const size_t es = (size_t)chi_cap * chi_cap;
-    double2 *L = envL + (size_t)blockIdx.x * (n + 1) * es;
-    double2 *Rv = envR + (size_t)blockIdx.x * (n + 1) * es;
+    double2 *L = envL + (size_t)chain * (n + 1) * es;
+    double2 *Rv = envR + (size_t)chain * (n + 1) * es;
     double2 *T = tscr + (size_t)blockIdx.x * 2 * es;
-    if (tid == 0) {
-        E[0] = make_double2(1.0, 0.0);
-        L[0] = E[0];
-    }
-    __syncthreads();
-    for (int k = 0; k < n; ++k) {
-        EnvStepArgs a{reinterpret_cast<const double2 *>(ch.sites + (size_t)k * ch.slot_elems), ch.bonds[k],
-                      ch.bonds[k + 1]};
-        left_step(E, a, nullptr, T, En, tid, nth);
-        trace_normalise(En, a.cr, red, tid, nth);
-        for (int e = tid; e < a.cr * a.cr; e += nth) {
-            E[e] = En[e];
-            L[(size_t)(k + 1) * es + e] = En[e];
+    if (left) {
+        if (tid == 0) {
+            E[0] = make_double2(1.0, 0.0);
+            L[0] = E[0];
         }
         __syncthreads();
+        for (int k = 0; k < n; ++k) {
+            EnvStepArgs a{reinterpret_cast<const double2 *>(ch.sites + (size_t)k * ch.slot_elems), ch.bonds[k],
+                          ch.bonds[k + 1]};
+            left_env_step_mma(E, a, T, En, gsm);
+            trace_normalise(En, a.cr, red, tid, nth);
+            for (int e = tid; e < a.cr * a.cr; e += nth) {
+                E[e] = En[e];
+                L[(size_t)(k + 1) * es + e] = En[e];
+            }
+            __syncthreads();
+        }
+        return;
     }
     if (tid == 0) {
         E[0] = make_double2(1.0, 0.0);
@@ -280,7 +324,7 @@ __global__ void environments_kernel(const mpsb_chain *chains, int n, int chi_cap
     for (int k = n - 1; k >= 0; --k) {
         EnvStepArgs a{reinterpret_cast<const double2 *>(ch.sites + (size_t)k * ch.slot_elems), ch.bonds[k],
                       ch.bonds[k + 1]};
-        right_step(E, a, T, En, tid, nth);
+        right_env_step_mma(E, a, T, En, gsm);
         trace_normalise(En, a.cl, red, tid, nth);
         for (int e = tid; e < a.cl * a.cl; e += nth) {
             E[e] = En[e];
@@ -375,7 +419,7 @@ __global__ void terms_kernel(const mpsb_chain *chains, int nchains, int n, int c
 
 size_t expect_workspace_bytes(int nchains, int n, int chi_cap, int nctas) {
     const size_t es = (size_t)chi_cap * chi_cap * sizeof(double2);
-    return (size_t)2 * nchains * (n + 1) * es + (size_t)nchains * 2 * es + (size_t)nctas * 4 * es;
+    return (size_t)2 * nchains * (n + 1) * es + (size_t)nchains * 4 * es + (size_t)nctas * 4 * es;
 }
 
 int launch_expect(const mpsb_chain *chains, int nchains, int n, int chi_cap, const int32_t *sites,
@@ -386,12 +430,12 @@ int launch_expect(const mpsb_chain *chains, int nchains, int n, int chi_cap, con
     double2 *envL = reinterpret_cast<double2 *>(ws);
     double2 *envR = envL + (size_t)nchains * (n + 1) * es;
     double2 *tscr = envR + (size_t)nchains * (n + 1) * es;
-    double2 *cscr = tscr + (size_t)nchains * 2 * es;
+    double2 *cscr = tscr + (size_t)nchains * 4 * es;  // 2 es of T per environment CTA, two CTAs per chain
     const size_t smem_env = 2 * es * sizeof(double2);
     int rc = ensure_smem(reinterpret_cast<const void *>(environments_kernel), smem_env,
                          "cudaFuncSetAttribute(environments)");
     if (rc) return rc;
-    environments_kernel<<<nchains, 256, smem_env, s>>>(chains, n, chi_cap, envL, envR, tscr);
+    environments_kernel<<<2 * nchains, 256, smem_env, s>>>(chains, n, chi_cap, envL, envR, tscr);
     rc = check_launch("environments_kernel");
     if (rc) return rc;
     const int grid = nchains * nterms < nctas ? nchains * nterms : nctas;
