@@ -484,6 +484,76 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- CPU side
+def contraction_leg(dev, batch, gates, steps: int, fp64_peak_tflops: float, update_s_per_update: float):
+    """theta = G (A B) alone (mpsb_contract2q_batch, the FPGA offload's piece), both forms,
+    on the finished config-2 state: its 99 adjacent pairs ten times over (990 thetas,
+    259 MB of output, larger than L2), device-timed per launch.  The tensor-core form is
+    held to a measured tcgen05 TF32 peak, the FP64 form to the FP64 probe."""
+    import torch
+    from fpga_mps_simulator_b200 import _lib
+    lib = _lib.load()
+    n = batch.ns[0]
+    reps = 10
+    sites = np.tile(np.arange(n - 1), reps)
+    tb = batch.make_thetas(np.zeros(len(sites), np.int32), sites, gates[: len(sites)])
+    bonds = batch.bonds.cpu().numpy()
+    dims = [(int(bonds[i]), int(bonds[i + 1]), int(bonds[i + 2])) for i in sites]
+    alg = float(sum(32.0 * cl * cm * cr + 128.0 * cl * cr for cl, cm, cr in dims))
+    # tensor-core flops the 3xTF32 complex-3M form issues: per CTA (two per pair, each
+    # half of the columns) 3 products x 3 MMAs per K = 8 step, M = 128 rows
+    issued = 0.0
+    for cl, cm, cr in dims:
+        w = ((2 * cr + 15) & ~15) >> 2
+        for half in (0, 1):
+            nidx = max(0, min(cr, half * w + w) - half * w)
+            if nidx:
+                npad = max(16, (2 * nidx + 15) & ~15)
+                issued += 9 * 2.0 * 128 * npad * ((cm + 7) & ~7)
+    s = torch.cuda.current_stream(dev)
+    res = {"pairs": len(sites), "flops_per_launch": alg, "workload": "config-2 final state, 99 pairs x 10"}
+    for form in ("fp64", "mixed"):
+        for _ in range(3):
+            batch.run_thetas(tb, form)
+        torch.cuda.synchronize()
+        if tb.status.any().item():
+            raise RuntimeError("contraction leg: a pair reported " + str(tb.status.cpu().numpy().max()))
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * steps)]
+        for k in range(steps):
+            ev[2 * k].record(s)
+            batch.run_thetas(tb, form)
+            ev[2 * k + 1].record(s)
+        torch.cuda.synchronize()
+        ms = float(np.mean([ev[2 * k].elapsed_time(ev[2 * k + 1]) for k in range(steps)]))
+        res[form] = {"ms_per_launch": round(ms, 4), "tflops": round(alg / (ms * 1e-3) / 1e12, 4),
+                     "us_per_theta": round(ms * 1e3 / len(sites), 4)}
+    # tcgen05 kind::tf32 peak: one CTA per SM, 16384 M128 N256 K8 MMAs each
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    sink = torch.zeros(sms, dtype=torch.float64, device=dev)
+    iters = 16384
+    for _ in range(2):
+        _lib.check(lib.mpsb_tf32_probe(iters, sms, sink.data_ptr(), s.cuda_stream), "tf32 probe")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    _lib.check(lib.mpsb_tf32_probe(iters, sms, sink.data_ptr(), s.cuda_stream), "tf32 probe")
+    e1.record(s)
+    torch.cuda.synchronize()
+    tf32_peak = 2.0 * 128 * 256 * 8 * iters * sms / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    mixed_s = res["mixed"]["ms_per_launch"] * 1e-3
+    res["mixed"].update({"tensor_tflops_issued": round(issued / mixed_s / 1e12, 4),
+                         "frac_of_tf32_peak": round(issued / mixed_s / 1e12 / tf32_peak, 5)})
+    res["fp64"]["frac_of_fp64_peak"] = round(res["fp64"]["tflops"] / fp64_peak_tflops, 5)
+    res["tf32_peak_tflops"] = round(tf32_peak, 3)
+    res["tf32_peak_source"] = "measured: tcgen05 kind::tf32 probe (mpsb_tf32_probe), one CTA per SM, burst"
+    res["share_of_an_update"] = {form: round(res[form]["us_per_theta"] * 1e-6 / update_s_per_update, 4)
+                                 for form in ("fp64", "mixed")}
+    res["note"] = ("tflops = algorithmic contraction+gate flops (32 chi_l chi_m chi_r + 128 chi_l chi_r per pair) "
+                   "per second; tensor_tflops_issued counts the 9 real TF32 GEMMs (3M x 3xTF32) with padding; "
+                   "share_of_an_update = theta time per pair / update time per pair in the per-layer launches "
+                   "(the update kernel runs the same code as its phase 1, two CTAs per pair)")
+    del tb
+    return res
+
+
 def cpu_baseline_sample(workers: int):
     from oracle.cpu_baseline import make_pool, run_parallel, single_process_default_threads
     pool = make_pool(workers)
@@ -722,6 +792,12 @@ def run_ours(args) -> None:
             b2.check_status()
         forms.clear()
 
+    # ---- the contraction alone (both forms) against its own rooflines
+    contraction = None
+    if not args.quick:
+        contraction = contraction_leg(dev, main["batch"], np.concatenate([L.gates for L in layers]), 5,
+                                      fp64_peak_tflops, main["kern_s"] / n_upd)
+
     # ---- the drop-in called gate by gate, as mps_core users write it (FP64): the whole
     # circuit as 990 MPSState._apply_adjacent_2q calls, then a read (flush), wall-clocked
     # from the first call to the synchronised result; deferred (default) and eager
@@ -837,6 +913,7 @@ def run_ours(args) -> None:
         "clocks": clk,
         "e2e": e2e,
         "per_update_path": single,
+        "contraction": contraction,
         "batching": batching,
         "gradient": gradient,
         "large": large,

@@ -9,7 +9,7 @@ __all__ = ["GATE_MATRICES", "SINGLE_QUBIT_GATES", "TWO_QUBIT_GATES", "gate_1q", 
 
 def __getattr__(name):
     # torch and the CUDA library are only needed for the device classes
-    if name in ("MPSState", "MPSBatch", "PairBatch", "FlowBatch"):
+    if name in ("MPSState", "MPSBatch", "PairBatch", "FlowBatch", "ThetaBatch"):
         from . import mps
         return getattr(mps, name)
     if name in ("MPSSimulator", "MPSResult", "Circuit"):

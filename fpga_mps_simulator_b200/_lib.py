@@ -37,6 +37,7 @@ EXPORTS = (
     "mpsb_mpo_energy_grad", "mpsb_sample_workspace_bytes", "mpsb_sample", "mpsb_reset_batch",
     "mpsb_canonicalize_workspace_bytes", "mpsb_canonicalize",
     "mpsb_update2q_flow_workspace_bytes", "mpsb_update2q_flow_clusters", "mpsb_update2q_flow",
+    "mpsb_contract2q_batch", "mpsb_tf32_probe",
 )
 
 # CTA sizes (threads) the dataflow kernel is built for, by rows per lane
@@ -99,6 +100,8 @@ def _declare(lib):
         "mpsb_expect_workspace_bytes": (sz, [i32, i32, i32]),
         "mpsb_expect_local": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp, vp, sz, vp]),
         "mpsb_fp64_probe": (i32, [i64, i32, i32, vp, vp]),
+        "mpsb_tf32_probe": (i32, [i64, i32, vp, vp]),
+        "mpsb_contract2q_batch": (i32, [vp, vp, i32, vp, i32, i32, vp, vp, vp]),
         "mpsb_update2q_batch_noalloc": (i32, [vp, vp, i32, vp, i32, i32, dbl, i32, vp, vp, vp, vp, vp]),
         "mpsb_overlap": (i32, [vp, vp, i32, i32, vp, vp, vp, sz, vp]),
         "mpsb_update2q_tape_bytes": (sz, [i32, i32]),

@@ -54,7 +54,7 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> str:
         subprocess.run(cmd, check=True)
     if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < _newest(objs):
         subprocess.run([nvcc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", LIB, *objs,
-                        "-lcudart"], check=True)
+                        "-lcudart", "-Xlinker", "-z,defs"], check=True)
     return LIB
 
 

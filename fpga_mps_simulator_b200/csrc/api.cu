@@ -87,6 +87,9 @@ size_t expect_workspace_bytes(int nchains, int n, int chi_cap, int nctas);
 int launch_expect(const mpsb_chain *, int, int, int, const int32_t *, const int32_t *, const double2 *, int,
                   double *, void *, int, cudaStream_t);
 int launch_fp64_probe(long long iters, int blocks, int threads, double *sink, cudaStream_t s);
+int launch_tf32_probe(long long iters, int blocks, double *sink, cudaStream_t s);
+int launch_theta2q(int, const mpsb_chain *, const mpsb_pair *, int, const double2 *, int, double2 *, int32_t *,
+                   cudaStream_t);
 int launch_overlap(const mpsb_chain *, const mpsb_chain *, int, int, double2 *, double *, void *, cudaStream_t);
 
 size_t upd_flow_workspace_bytes(int nitems, int chi_cap, int precision, int threads, int nclusters);
@@ -199,6 +202,21 @@ int mpsb_update2q_flow(const mpsb_chain *chains, int nchains, const mpsb_flow_it
                                 reinterpret_cast<const double2 *>(gates), precision, chi_cap, tol, max_sweeps,
                                 threads, nclusters, poll_limit, workspace, workspace_bytes, spectra, kept, trunc,
                                 status, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mpsb_contract2q_batch(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs, const mpsb_c128 *gates,
+                          int precision, int chi_cap, mpsb_c128 *theta, int32_t *status, mpsb_stream_t stream) {
+    if (npairs < 0) return set_error(MPSB_EINVAL, "npairs=%d < 0", npairs);
+    if (npairs == 0) return MPSB_OK;
+    if (!chains || !pairs || !gates || !theta || !status)
+        return set_error(MPSB_EINVAL, "null chains/pairs/gates/theta/status pointer");
+    if (chi_cap < 1 || chi_cap > MPSB_CHI_LIMIT)
+        return set_error(MPSB_EINVAL, "chi_cap=%d outside [1, %d]", chi_cap, MPSB_CHI_LIMIT);
+    if (!valid_precision(precision)) return set_error(MPSB_EINVAL, "unknown precision %d", precision);
+    int rc = check_device(chains, stream);
+    if (rc) return rc;
+    return launch_theta2q(precision, chains, pairs, npairs, reinterpret_cast<const double2 *>(gates), chi_cap,
+                          reinterpret_cast<double2 *>(theta), status, reinterpret_cast<cudaStream_t>(stream));
 }
 
 int mpsb_apply1q_batch(const mpsb_chain *chains, const mpsb_site_op *ops, int nops, const mpsb_c128 *gates,
@@ -438,6 +456,15 @@ int mpsb_fp64_probe(int64_t iters, int blocks, int threads, double *sink, mpsb_s
     int rc = check_device(nullptr, stream);
     if (rc) return rc;
     return launch_fp64_probe(iters, blocks, threads, sink, reinterpret_cast<cudaStream_t>(stream));
+}
+
+int mpsb_tf32_probe(int64_t iters, int blocks, double *sink, mpsb_stream_t stream) {
+    // (the cap keeps one CTA's MMA chain, ~5 ms at the TF32 peak, far inside
+    // the bounded completion wait)
+    if (iters < 1 || iters > 65536 || blocks < 1 || !sink) return set_error(MPSB_EINVAL, "bad probe arguments");
+    int rc = check_device(nullptr, stream);
+    if (rc) return rc;
+    return launch_tf32_probe(iters, blocks, sink, reinterpret_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

@@ -961,6 +961,82 @@ __device__ __forceinline__ double2 ld_site(const double2 *p) {
         return __ldg(p);
 }
 
+// Phase 1 of an update, also the whole of the contraction-only kernel:
+// theta = G (A B) for this CTA's share [idx0, idx0 + nidx) of the split index
+// (d when X = M, a when X = M^H), written into the Jacobi slots X (shared
+// memory) and into x0 as the R x C row-major matrix X.  The gate is read from
+// sc->gate; a non-finite entry sets sc->nonfinite, a tensor-core wait that
+// gave up sets sc->timeout.  FP64 form: the slots must be zero beforehand.
+template <int NT, bool MIXED, bool FLOW>
+__device__ __forceinline__ void form_theta(CtaScalars *sc, double2 *X, const double2 *A, const double2 *B, int cl,
+                                           int cm, int cr, bool trans, int idx0, int nidx, int C, int w, int wmax,
+                                           int rpad, double2 *x0, int tid) {
+    if constexpr (MIXED) {
+        int nonfin = 0;
+        const bool ok = contract_mixed<NT, FLOW>(reinterpret_cast<unsigned char *>(X), &sc->mbar, &sc->tmem, A, B,
+                                                 sc->gate, cl, cm, cr, trans, idx0, nidx, C, w, wmax, rpad, X, x0,
+                                                 tid, nonfin);
+        if (nonfin) atomicOr(&sc->nonfinite, 1);
+        if (!ok && tid == 0) sc->timeout = 1;
+        __threadfence();
+    } else {
+        const double2 *g = sc->gate;
+        const int other = trans ? cr : cl;
+        const int total = nidx * other;
+        int nonfin = 0;
+        for (int e = tid; e < total; e += NT) {
+            int a, d;
+            if (!trans) {
+                a = e / nidx;
+                d = idx0 + (e - a * nidx);
+            } else {
+                const int q = e / cr;
+                a = idx0 + q;
+                d = e - q * cr;
+            }
+            double2 t00 = make_double2(0, 0), t01 = t00, t10 = t00, t11 = t00;
+            const double2 *ap0 = A + (size_t)(2 * a) * cm;
+            const double2 *ap1 = ap0 + cm;
+            const double2 *bp = B + d;
+            for (int b = 0; b < cm; ++b) {
+                const double2 a0 = ld_site<FLOW>(ap0 + b), a1 = ld_site<FLOW>(ap1 + b);
+                const double2 b0 = ld_site<FLOW>(bp + (size_t)(2 * b) * cr);
+                const double2 b1 = ld_site<FLOW>(bp + (size_t)(2 * b + 1) * cr);
+                t00 = c_fma(a0, b0, t00);
+                t01 = c_fma(a0, b1, t01);
+                t10 = c_fma(a1, b0, t10);
+                t11 = c_fma(a1, b1, t11);
+            }
+#pragma unroll
+            for (int s0 = 0; s0 < 2; ++s0) {
+#pragma unroll
+                for (int s1 = 0; s1 < 2; ++s1) {
+                    const int s = 2 * s0 + s1;
+                    double2 m = c_mul(g[4 * s + 0], t00);
+                    m = c_fma(g[4 * s + 1], t01, m);
+                    m = c_fma(g[4 * s + 2], t10, m);
+                    m = c_fma(g[4 * s + 3], t11, m);
+                    nonfin |= !c_finite(m);
+                    if (!trans) {
+                        const int r = 2 * a + s0, j = 2 * (d - idx0) + s1;
+                        const int slot = j >= w, jj = j - slot * w;
+                        X[(size_t)(slot * wmax + jj) * rpad + r] = m;
+                        x0[(size_t)r * C + s1 * cr + d] = m;
+                    } else {
+                        const int r = s1 * cr + d, j = 2 * (a - idx0) + s0;
+                        const int slot = j >= w, jj = j - slot * w;
+                        const double2 mc = c_conj(m);
+                        X[(size_t)(slot * wmax + jj) * rpad + r] = mc;
+                        x0[(size_t)r * C + 2 * a + s0] = mc;
+                    }
+                }
+            }
+        }
+        if (nonfin) atomicOr(&sc->nonfinite, 1);
+        __threadfence();
+    }
+}
+
 // One two-site update by the calling cluster: pair `pr` (row `pi` of the
 // per-pair records), unrotated theta kept at x0 (this pair's workspace
 // region).  Both CTAs of the cluster call it with the same arguments; it ends
@@ -1030,75 +1106,10 @@ __device__ __forceinline__ void update_pair(const Upd2Params &p, const int pi, c
     __syncthreads();
 
     // ---- phase 1: theta for this CTA's columns, into X (smem) and X0 (workspace)
-    if constexpr (MIXED) {
+    {
         const double2 *A = reinterpret_cast<const double2 *>(ch.sites + (size_t)i * ch.slot_elems);
         const double2 *B = reinterpret_cast<const double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
-        double2 *x0 = x0pair;
-        int nonfin = 0;
-        const bool ok = contract_mixed<NT, FLOW>(reinterpret_cast<unsigned char *>(X), &sc->mbar, &sc->tmem, A, B,
-                                                 sc->gate, cl, cm, cr, trans, idx0, nidx, C, w, wmax, rpad, X, x0,
-                                                 tid, nonfin);
-        if (nonfin) atomicOr(&sc->nonfinite, 1);
-        if (!ok && tid == 0) sc->timeout = 1;
-        __threadfence();
-    } else {
-        const double2 *g = sc->gate;
-        const double2 *A = reinterpret_cast<const double2 *>(ch.sites + (size_t)i * ch.slot_elems);
-        const double2 *B = reinterpret_cast<const double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
-        double2 *x0 = x0pair;
-        const int other = trans ? cr : cl;
-        const int total = nidx * other;
-        int nonfin = 0;
-        for (int e = tid; e < total; e += kUpdThreads) {
-            int a, d;
-            if (!trans) {
-                a = e / nidx;
-                d = idx0 + (e - a * nidx);
-            } else {
-                const int q = e / cr;
-                a = idx0 + q;
-                d = e - q * cr;
-            }
-            double2 t00 = make_double2(0, 0), t01 = t00, t10 = t00, t11 = t00;
-            const double2 *ap0 = A + (size_t)(2 * a) * cm;
-            const double2 *ap1 = ap0 + cm;
-            const double2 *bp = B + d;
-            for (int b = 0; b < cm; ++b) {
-                const double2 a0 = ld_site<FLOW>(ap0 + b), a1 = ld_site<FLOW>(ap1 + b);
-                const double2 b0 = ld_site<FLOW>(bp + (size_t)(2 * b) * cr);
-                const double2 b1 = ld_site<FLOW>(bp + (size_t)(2 * b + 1) * cr);
-                t00 = c_fma(a0, b0, t00);
-                t01 = c_fma(a0, b1, t01);
-                t10 = c_fma(a1, b0, t10);
-                t11 = c_fma(a1, b1, t11);
-            }
-#pragma unroll
-            for (int s0 = 0; s0 < 2; ++s0) {
-#pragma unroll
-                for (int s1 = 0; s1 < 2; ++s1) {
-                    const int s = 2 * s0 + s1;
-                    double2 m = c_mul(g[4 * s + 0], t00);
-                    m = c_fma(g[4 * s + 1], t01, m);
-                    m = c_fma(g[4 * s + 2], t10, m);
-                    m = c_fma(g[4 * s + 3], t11, m);
-                    nonfin |= !c_finite(m);
-                    if (!trans) {
-                        const int r = 2 * a + s0, j = 2 * (d - idx0) + s1;
-                        const int slot = j >= w, jj = j - slot * w;
-                        X[(size_t)(slot * wmax + jj) * rpad + r] = m;
-                        x0[(size_t)r * C + s1 * cr + d] = m;
-                    } else {
-                        const int r = s1 * cr + d, j = 2 * (a - idx0) + s0;
-                        const int slot = j >= w, jj = j - slot * w;
-                        const double2 mc = c_conj(m);
-                        X[(size_t)(slot * wmax + jj) * rpad + r] = mc;
-                        x0[(size_t)r * C + 2 * a + s0] = mc;
-                    }
-                }
-            }
-        }
-        if (nonfin) atomicOr(&sc->nonfinite, 1);
-        __threadfence();
+        form_theta<NT, MIXED, FLOW>(sc, X, A, B, cl, cm, cr, trans, idx0, nidx, C, w, wmax, rpad, x0pair, tid);
     }
     __syncthreads();
 
@@ -1648,6 +1659,167 @@ int launch_update2q(int precision, const mpsb_chain *chains, const mpsb_pair *pa
                     int32_t *kept, double *trunc, int32_t *status, cudaStream_t stream) {
     return launch_update2q_impl(precision, chains, pairs, npairs, gates, chi_cap, tol, max_sweeps, ws, spectra, kept,
                                 trunc, status, stream);
+}
+
+// ------------------------------------------------------- contraction only
+// theta = G (A B) of each pair, returned as the (2 chi_l) x (2 chi_r)
+// row-major matrix M = theta[a][s][d] -- the device half of the reference's
+// FPGA offload (contract_and_apply_2q, fpga_mps_simulator.cpp:287-371, whose
+// output the host reads back as a (2 chi_l, 2 chi_r) matrix for its SVD,
+// fpga_mps_simulator.py:597-600).  Two independent CTAs per pair, each
+// forming half of the columns with phase 1 of the update (form_theta, never
+// transposed), so an FP64 theta is bitwise the one the update factorises.
+constexpr int kThetaThreads = 256;
+
+struct ThetaParams {
+    const mpsb_chain *chains;
+    const mpsb_pair *pairs;
+    const double2 *gates;
+    double2 *theta;   // pair k's matrix at theta + pairs[k].out * (2 chi_cap)^2, leading dimension 2 chi_r
+    int32_t *status;  // per pairs[k].out: bits or-ed in (cleared by theta_clear_kernel first)
+    int chi_cap;
+    int wmax, rpad;
+};
+
+__global__ void theta_clear_kernel(const mpsb_pair *pairs, int npairs, int32_t *status) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < npairs) status[pairs[k].out] = 0;
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(kThetaThreads, 1) theta2q_kernel(ThetaParams p) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int pi = blockIdx.x >> 1, half = blockIdx.x & 1, tid = threadIdx.x;
+    CtaScalars *sc = reinterpret_cast<CtaScalars *>(smem_raw);
+    double2 *X = reinterpret_cast<double2 *>(smem_raw + 384);
+    const mpsb_pair pr = p.pairs[pi];
+    const mpsb_chain ch = p.chains[pr.chain];
+    const int i = pr.site;
+    bool bad = i < 0 || i + 2 > ch.n;
+    int cl = 0, cm = 0, cr = 0;
+    if (!bad) {
+        cl = ch.bonds[i];
+        cm = ch.bonds[i + 1];
+        cr = ch.bonds[i + 2];
+        bad = cl < 1 || cm < 1 || cr < 1 || cl > p.chi_cap || cm > p.chi_cap || cr > p.chi_cap;
+    }
+    if (bad) {
+        if (half == 0 && tid == 0) atomicOr(p.status + pr.out, MPSB_ST_BADDIM);
+        return;
+    }
+    const int C = 2 * cr;
+    const int w = ((C + 15) & ~15) >> 2;
+    const int idx0 = half * w;
+    const int nidx = max(0, min(cr, idx0 + w) - idx0);
+    if (nidx == 0) return;  // (the whole CTA: a narrow theta fits in the first half)
+    if (tid == 0) {
+        sc->nonfinite = 0;
+        sc->timeout = 0;
+    }
+    if (tid < 16) sc->gate[tid] = __ldg(p.gates + (size_t)pr.gate * 16 + tid);
+    __syncthreads();
+    const double2 *A = reinterpret_cast<const double2 *>(ch.sites + (size_t)i * ch.slot_elems);
+    const double2 *B = reinterpret_cast<const double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
+    double2 *x0 = p.theta + (size_t)pr.out * (size_t)(2 * p.chi_cap) * (size_t)(2 * p.chi_cap);
+    form_theta<kThetaThreads, MIXED, false>(sc, X, A, B, cl, cm, cr, false, idx0, nidx, C, w, p.wmax, p.rpad, x0,
+                                            tid);
+    __syncthreads();
+    if (tid == 0) {
+        const int flags = (sc->nonfinite ? MPSB_ST_NONFINITE : 0) | (sc->timeout ? MPSB_ST_TIMEOUT : 0);
+        if (flags) atomicOr(p.status + pr.out, flags);
+    }
+}
+
+int launch_theta2q(int precision, const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+                   const double2 *gates, int chi_cap, double2 *theta, int32_t *status, cudaStream_t stream) {
+    if (npairs == 0) return MPSB_OK;
+    ThetaParams p;
+    p.chains = chains;
+    p.pairs = pairs;
+    p.gates = gates;
+    p.theta = theta;
+    p.status = status;
+    p.chi_cap = chi_cap;
+    const int rpl = (2 * chi_cap <= 32) ? 1 : (2 * chi_cap <= 64) ? 2 : 4;
+    p.rpad = 32 * rpl;
+    p.wmax = (((2 * chi_cap) + 15) & ~15) / 4;
+    // the same contraction as the update of this precision and cap
+    bool mixed = precision != MPSB_FP64;
+    if (precision == MPSB_MIXED_TF32X3 && rpl <= 2) mixed = false;
+    size_t smem = 384 + (size_t)2 * p.wmax * p.rpad * sizeof(double2);
+    if (mixed) {
+        smem = upd_smem_bytes_mixed(p.wmax, p.rpad, chi_cap);
+        // at most four resident CTAs per SM, so that their TMEM (<= 128
+        // columns each at chi_cap <= 32; 256 above, where the shared memory
+        // allows one CTA per SM) always fits in the SM's 512 columns
+        if (smem < 57344) smem = 57344;
+    }
+    theta_clear_kernel<<<(npairs + 255) / 256, 256, 0, stream>>>(pairs, npairs, status);
+    int rc = check_launch("theta_clear_kernel");
+    if (rc) return rc;
+    const void *fn = mixed ? reinterpret_cast<const void *>(theta2q_kernel<true>)
+                           : reinterpret_cast<const void *>(theta2q_kernel<false>);
+    rc = ensure_smem(fn, smem, "cudaFuncSetAttribute(theta2q)");
+    if (rc) return rc;
+    if (mixed)
+        theta2q_kernel<true><<<2 * npairs, kThetaThreads, smem, stream>>>(p);
+    else
+        theta2q_kernel<false><<<2 * npairs, kThetaThreads, smem, stream>>>(p);
+    return check_launch("theta2q kernel");
+}
+
+// ------------------------------------------------------- TF32 tensor peak
+// Dense kind::tf32 tcgen05 throughput, the roofline denominator of the
+// tensor-core contraction: each CTA keeps one M = 128, N = 256 fp32
+// accumulator in TMEM and one thread issues `iters` MMAs (K = 8) on fixed
+// operand tiles, 2 * 128 * 256 * 8 flops each.  The unused dynamic shared
+// memory of the launch keeps it at one CTA per SM.
+constexpr int kProbeM = 128, kProbeN = 256, kProbeK = 8;
+constexpr size_t kProbeSmem = 120 * 1024;
+
+__global__ void __launch_bounds__(128, 1) tf32_probe_kernel(long long iters, double *sink) {
+    __shared__ __align__(128) uint32_t a_tile[kProbeM * kProbeK];
+    __shared__ __align__(128) uint32_t b_tile[kProbeN * kProbeK];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tslot;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < kProbeM * kProbeK; e += 128) a_tile[e] = tc::to_tf32(1.0f / 64);
+    for (int e = tid; e < kProbeN * kProbeK; e += 128) b_tile[e] = tc::to_tf32(1.0f / 128);
+    if ((tid >> 5) == 0) tc::tmem_alloc(&tslot, 256);
+    if (tid == 0) {
+        tc::mbar_init(&mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = tslot;
+    if (tid == 0) {
+        // canonical K-major layout at K = 8: the two 16-byte K chunks of a row
+        // group 128 B apart, 8-row groups 256 B apart
+        const uint32_t idesc = tc::make_idesc_tf32(kProbeM, kProbeN);
+        const uint64_t ad = tc::make_desc(tc::smem_u32(a_tile), 128, 256);
+        const uint64_t bd = tc::make_desc(tc::smem_u32(b_tile), 128, 256);
+        for (long long it = 0; it < iters; ++it) tc::mma_tf32(tmem, ad, bd, idesc, it > 0 ? 1u : 0u);
+        tc::mma_commit(&mbar);
+    }
+    const bool ok = tc::mbar_wait(&mbar, 0);
+    tc::fence_after_sync();
+    float v[16];
+    tc::tmem_ld16(tmem + (static_cast<uint32_t>(32 * (tid >> 5)) << 16), v);
+    if (tid == 0) sink[blockIdx.x] = ok ? static_cast<double>(v[0]) : -1.0;
+    tc::fence_before_sync();
+    __syncthreads();
+    if ((tid >> 5) == 0) tc::tmem_free(tmem, 256);
+}
+
+int launch_tf32_probe(long long iters, int blocks, double *sink, cudaStream_t s) {
+    const int rc = ensure_smem(reinterpret_cast<const void *>(tf32_probe_kernel), kProbeSmem,
+                               "cudaFuncSetAttribute(tf32_probe)");
+    if (rc) return rc;
+    tf32_probe_kernel<<<blocks, 128, kProbeSmem, s>>>(iters, sink);
+    return check_launch("tf32_probe_kernel");
 }
 
 // ------------------------------------------------------- persistent launcher

@@ -204,6 +204,50 @@ class FlowBatch:
         self.gates.copy_(torch.from_numpy(np.ascontiguousarray(g.reshape(self.nitems, 16))))
 
 
+class ThetaBatch:
+    """Device tables for one contraction-only launch (``MPSBatch.run_thetas``).
+
+    Pair k is (chain_idx[k], sites[k]) with gate k; pairs only read the sites,
+    so they may overlap.  ``theta`` holds one (2 chi_cap)^2 row per pair: the
+    (2 chi_l) x (2 chi_r) matrix, row-major, at its start.  Reusable across
+    launches and CUDA-graph replays.
+    """
+
+    def __init__(self, owner: "MPSBatch", chain_idx, sites, gates):
+        chain_idx = np.asarray(chain_idx, np.int64).reshape(-1)
+        sites = np.asarray(sites, np.int64).reshape(-1)
+        g = np.asarray(gates, dtype=np.complex128).reshape(-1, 16)
+        if not (len(chain_idx) == len(sites) == len(g)):
+            raise ValueError("chain_idx, sites and gates must have one entry per pair")
+        P = len(sites)
+        if P and (np.any(chain_idx < 0) or np.any(chain_idx >= owner.nchains)):
+            raise ValueError("pair chain index out of range")
+        if P and (np.any(sites < 0) or np.any(sites + 1 >= np.asarray(owner.ns, np.int64)[chain_idx])):
+            raise ValueError("pair site out of range: need 0 <= i and i + 1 < n")
+        dev = owner.device
+        self.owner = owner
+        self.npairs = P
+        self.chain_idx = chain_idx
+        self.sites = sites
+        table = np.stack([chain_idx, sites, np.arange(P), np.arange(P)], 1).astype(np.int32)
+        self.pairs = torch.from_numpy(np.ascontiguousarray(table)).to(dev)
+        self.gates = torch.from_numpy(np.ascontiguousarray(g)).to(dev)
+        self.status = torch.zeros(P, dtype=torch.int32, device=dev)
+        self.theta = torch.zeros(P, (2 * owner.chi_cap) ** 2, dtype=torch.complex128, device=dev)
+
+    def matrices(self) -> List[np.ndarray]:
+        """Host copies of the thetas, each (2 chi_l, 2 chi_r), from the current bonds."""
+        th = self.theta.cpu().numpy()
+        bonds = self.owner.bonds.cpu().numpy()
+        out = []
+        for k in range(self.npairs):
+            c, i = int(self.chain_idx[k]), int(self.sites[k])
+            b0 = int(self.owner.bond_off[c])
+            cl, cr = int(bonds[b0 + i]), int(bonds[b0 + i + 2])
+            out.append(th[k, : 4 * cl * cr].reshape(2 * cl, 2 * cr).copy())
+        return out
+
+
 class MPSBatch:
     """Independent chains in one device allocation.
 
@@ -319,6 +363,37 @@ class MPSBatch:
             cap, self.tol, self.max_sweeps, ws.data_ptr(), ws.numel(),
             _ptr(pb.spectra), pb.kept.data_ptr(), pb.trunc.data_ptr(), pb.status.data_ptr(), handle)
         _lib.check(rc, "mpsb_update2q_batch")
+
+    def make_thetas(self, chain_idx, sites, gates) -> ThetaBatch:
+        return ThetaBatch(self, chain_idx, sites, gates)
+
+    def run_thetas(self, tb: ThetaBatch, precision: Optional[str] = None,
+                   stream: Optional[torch.cuda.Stream] = None) -> None:
+        """theta = G (A B) of every pair of ``tb``, no SVD (asynchronous, stream-ordered).
+
+        The contraction the update of ``precision`` runs at this batch's bond
+        cap (``mpsb_contract2q_batch``): the device half of the reference's
+        FPGA offload, fpga_mps_simulator.cpp:287-371.  Status bits per pair
+        land in ``tb.status``.
+        """
+        if tb.npairs == 0:
+            return
+        prec = PRECISIONS[precision or self.precision]
+        handle = (stream or torch.cuda.current_stream(self.device)).cuda_stream
+        rc = self._lib.mpsb_contract2q_batch(
+            self.table.data_ptr(), tb.pairs.data_ptr(), tb.npairs, tb.gates.data_ptr(), prec, self.chi_cap,
+            tb.theta.data_ptr(), tb.status.data_ptr(), handle)
+        _lib.check(rc, "mpsb_contract2q_batch")
+
+    def thetas(self, chain_idx, sites, gates, precision: Optional[str] = None) -> List[np.ndarray]:
+        """Host thetas, (2 chi_l, 2 chi_r) each, of the given pairs (synchronous)."""
+        tb = self.make_thetas(chain_idx, sites, gates)
+        self.run_thetas(tb, precision)
+        st = tb.status.cpu().numpy()
+        if np.any(st):
+            raise RuntimeError("contraction failed: " + "; ".join(
+                f"pair {k}: {_lib.status_text(int(v))}" for k, v in enumerate(st) if v))
+        return tb.matrices()
 
     def make_flow(self, chain_idx, sites, gates, record_spectra: bool = False) -> FlowBatch:
         return FlowBatch(self, chain_idx, sites, gates, record_spectra)
@@ -729,6 +804,16 @@ class MPSState:
             self.flush()
 
     apply_adjacent_2q = _apply_adjacent_2q
+
+    def theta(self, i: int, gate: np.ndarray) -> np.ndarray:
+        """theta = G (A_i A_{i+1}) as the (2 chi_l, 2 chi_r) matrix the update would
+        factorise, without applying it: what the reference's FPGA kernel returns
+        for its host SVD (fpga_mps_simulator.py:584-600)."""
+        i = int(i)
+        if not 0 <= i < self.n - 1:
+            raise ValueError(f"pair site out of range: need 0 <= i and i + 1 < n, got i={i}, n={self.n}")
+        g = np.array(gate, dtype=np.complex128).reshape(1, 4, 4)
+        return self._b.thetas([0], [i], g)[0]
 
     def apply_2q(self, i: int, j: int, gate: np.ndarray) -> None:
         """Dispatch of mps_core.py:304-324, including its SWAP routing.

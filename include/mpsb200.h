@@ -205,6 +205,26 @@ MPSB_API int mpsb_update2q_flow(const mpsb_chain *chains, int nchains, const mps
                                 double *spectra, int32_t *kept, double *trunc, int32_t *status,
                                 mpsb_stream_t stream);
 
+/* Contraction only: theta = G (A B) of each pair, without the SVD -- the work
+ * of the reference's FPGA offload (contract_and_apply_2q,
+ * fpga_mps_simulator.cpp:287-371, opcode 100 of its instruction stream) whose
+ * result the host reads back as the (2 chi_l) x (2 chi_r) matrix
+ * theta[a][s][d] for its own SVD (fpga_mps_simulator.py:597-600).
+ *   theta:  device, complex128; pair k's matrix, row-major with leading
+ *           dimension 2 * chi_r, starts at theta + pairs[k].out * (2 chi_cap)^2.
+ *   status: device int32 per pairs[k].out: MPSB_ST_BADDIM, MPSB_ST_NONFINITE,
+ *           MPSB_ST_TIMEOUT (cleared by the call).
+ * precision: the contraction the update of that precision runs at this
+ * chi_cap (FP64; 3xTF32 tensor cores for MPSB_MIXED_TF32X3 above chi_cap 32
+ * and for MPSB_TF32X3_ALL), so an FP64 theta is bitwise the matrix
+ * mpsb_update2q_batch factorises.  Gates are complex128 (the FPGA driver
+ * rounds them to float32 first; mps_core does not).  Sites are only read, so
+ * pairs may overlap; their `out` rows must be distinct.  Stream-ordered, no
+ * host synchronisation. */
+MPSB_API int mpsb_contract2q_batch(const mpsb_chain *chains, const mpsb_pair *pairs, int npairs,
+                                   const mpsb_c128 *gates, int precision, int chi_cap, mpsb_c128 *theta,
+                                   int32_t *status, mpsb_stream_t stream);
+
 /* Batched single-site gates, A'[l,s',r] = sum_s G[s',s] A[l,s,r], in place
  * (mps_core.py:267-273; fpga_mps_simulator.cpp:232-276 apply_1q_gate).
  * Ops of one call must touch distinct sites. */
@@ -363,6 +383,14 @@ MPSB_API int mpsb_mpo_energy_grad(const mpsb_chain *chains, int nchains, int n, 
  * The caller times the launch on `stream` to state the FP64 roofline.
  * sink: device, one double (written only to keep the chains live). */
 MPSB_API int mpsb_fp64_probe(int64_t iters, int blocks, int threads, double *sink, mpsb_stream_t stream);
+
+/* Dense TF32 tensor-core throughput probe (tcgen05.mma kind::tf32): `blocks`
+ * CTAs, one per SM, each issue `iters` (1 .. 65536) M = 128, N = 256, K = 8
+ * MMAs into one TMEM accumulator (2 * 128 * 256 * 8 * iters flops per CTA).
+ * The caller times the launch on `stream` to state the tensor roofline of
+ * the 3xTF32 contraction.  sink: device, `blocks` doubles (an accumulator
+ * value, or -1 where the completion wait gave up). */
+MPSB_API int mpsb_tf32_probe(int64_t iters, int blocks, double *sink, mpsb_stream_t stream);
 
 #ifdef __cplusplus
 }
