@@ -895,7 +895,7 @@ def run_ours(args) -> None:
                                                          if single else None),
             "target": ">= 5x the plain complex128 GPU form at infidelity <= 1e-6",
             "note": ("first reading: both forms batched, one dataflow launch each (the mixed form moves only the "
-                     "~5 % contraction share of an update onto the tensor cores; the FP64 Jacobi SVD is the rest); "
+                     "contraction, 1-2 % of an update (the contraction leg), onto the tensor cores; the FP64 Jacobi SVD is the rest); "
                      "second reading: the plain form as the drop-in runs it one update per launch; third: the "
                      "drop-in called gate by gate with its calls queued into one dataflow launch")},
         "data": "synthetic (seeded Haar-random 4x4 gates, |0...0> start)",
@@ -932,6 +932,17 @@ def run_leg(args) -> None:
         res = gradient_leg(dev, args.steps, args.warmup, 0, ident)
     elif args.leg == "batching":
         res = batching_leg(dev, args.steps, 0, ident)
+    elif args.leg == "contraction":
+        from fpga_mps_simulator_b200 import MPSBatch
+        from fpga_mps_simulator_b200.circuits import brickwall_layers
+        layers = brickwall_layers(N_SITES, DEPTH, SEED)
+        batch = MPSBatch([N_SITES], [CHI], [CUTOFF], precision="mixed", device=dev)
+        for L in layers:
+            batch.apply_layer(np.zeros(len(L.sites), np.int32), L.sites, L.gates)
+        torch.cuda.synchronize()
+        batch.check_status()
+        res = contraction_leg(dev, batch, np.concatenate([L.gates for L in layers]), args.steps, float("nan"),
+                              float("nan"))
     else:
         res = large_leg(dev)
     print(json.dumps({"leg": args.leg, **res}), flush=True)
@@ -951,7 +962,7 @@ def main():
                     help="Jacobi off-diagonal tolerance of the mixed form (0 = library default 1e-9)")
     ap.add_argument("--no-batching", action="store_true", help="skip the 256-circuit batching leg")
     ap.add_argument("--no-gradient", action="store_true", help="skip the ansatz energy-gradient leg")
-    ap.add_argument("--leg", choices=["all", "gradient", "batching", "large"], default="all",
+    ap.add_argument("--leg", choices=["all", "gradient", "batching", "large", "contraction"], default="all",
                     help="run one secondary leg alone and print its JSON (profiling)")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the 1000-qubit XXZ initial-state gradient leg (about a minute)")
