@@ -229,7 +229,7 @@ __device__ __forceinline__ void issue_product(unsigned char *buf, uint32_t tmem,
 // or, in lanes 0..15, rows m = 16 (w & 3) + lane (M = 64).  The two values of
 // a row pair (m, m ^ 1) meet by shuffle.  Rows no warp reads (M = 64 with two
 // warps: rows 32..63) must be padding (mvalid <= 32).
-template <int NT>
+template <int NT, bool WRITE_X = true>
 __device__ void read_theta(uint32_t tmem, const TcShape &sh, const double2 *g, bool trans, int cr, int C,
                            int idx0, int nidx, int w, int wmax, int rpad, double2 *X, double2 *x0, int tid,
                            int &nonfin) {
@@ -290,7 +290,7 @@ __device__ void read_theta(uint32_t tmem, const TcShape &sh, const double2 *g, b
                     v = c_conj(v);
                 }
                 const int slot = j >= w, jl = j - slot * w;
-                X[(size_t)(slot * wmax + jl) * rpad + r] = v;
+                if constexpr (WRITE_X) X[(size_t)(slot * wmax + jl) * rpad + r] = v;
                 x0[(size_t)r * C + xcol] = v;
             }
         }
@@ -302,7 +302,9 @@ __device__ void read_theta(uint32_t tmem, const TcShape &sh, const double2 *g, b
 // released on every path.  Called once per CTA (a CTA may allocate TMEM
 // only until it relinquishes the permit).  COHERENT: read the sites through
 // L2 (the dataflow kernel, where other clusters of the launch wrote them).
-template <int NT, bool COHERENT = false>
+// WRITE_X = false (the contraction-only kernel): theta goes to x0 alone, so
+// the shared memory holds just the operand staging area.
+template <int NT, bool COHERENT = false, bool WRITE_X = true>
 __device__ bool contract_mixed(unsigned char *opbuf, uint64_t *mbar, uint32_t *tmem_slot, const double2 *A,
                                const double2 *B, const double2 *g, int cl, int cm, int cr, bool trans, int idx0,
                                int nidx, int C, int w, int wmax, int rpad, double2 *X, double2 *x0, int tid,
@@ -339,9 +341,10 @@ __device__ bool contract_mixed(unsigned char *opbuf, uint64_t *mbar, uint32_t *t
     }
     tc::fence_after_sync();
     // the operand staging area overlaps the Jacobi slots: clear them before writing theta
-    for (int e = tid; e < 2 * wmax * rpad; e += NT) X[e] = make_double2(0.0, 0.0);
+    if constexpr (WRITE_X)
+        for (int e = tid; e < 2 * wmax * rpad; e += NT) X[e] = make_double2(0.0, 0.0);
     __syncthreads();
-    if (ok) read_theta<NT>(tmem, sh, g, trans, cr, C, idx0, nidx, w, wmax, rpad, X, x0, tid, nonfin);
+    if (ok) read_theta<NT, WRITE_X>(tmem, sh, g, trans, cr, C, idx0, nidx, w, wmax, rpad, X, x0, tid, nonfin);
     tc::fence_before_sync();
     __syncthreads();
     if ((tid >> 5) == 0) tc::tmem_free(tmem, ncols);

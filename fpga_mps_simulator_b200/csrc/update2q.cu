@@ -967,15 +967,16 @@ __device__ __forceinline__ double2 ld_site(const double2 *p) {
 // memory) and into x0 as the R x C row-major matrix X.  The gate is read from
 // sc->gate; a non-finite entry sets sc->nonfinite, a tensor-core wait that
 // gave up sets sc->timeout.  FP64 form: the slots must be zero beforehand.
-template <int NT, bool MIXED, bool FLOW>
+// WRITE_X = false: x0 only (the contraction-only kernel; X is not touched).
+template <int NT, bool MIXED, bool FLOW, bool WRITE_X = true>
 __device__ __forceinline__ void form_theta(CtaScalars *sc, double2 *X, const double2 *A, const double2 *B, int cl,
                                            int cm, int cr, bool trans, int idx0, int nidx, int C, int w, int wmax,
                                            int rpad, double2 *x0, int tid) {
     if constexpr (MIXED) {
         int nonfin = 0;
-        const bool ok = contract_mixed<NT, FLOW>(reinterpret_cast<unsigned char *>(X), &sc->mbar, &sc->tmem, A, B,
-                                                 sc->gate, cl, cm, cr, trans, idx0, nidx, C, w, wmax, rpad, X, x0,
-                                                 tid, nonfin);
+        const bool ok = contract_mixed<NT, FLOW, WRITE_X>(reinterpret_cast<unsigned char *>(X), &sc->mbar,
+                                                          &sc->tmem, A, B, sc->gate, cl, cm, cr, trans, idx0, nidx,
+                                                          C, w, wmax, rpad, X, x0, tid, nonfin);
         if (nonfin) atomicOr(&sc->nonfinite, 1);
         if (!ok && tid == 0) sc->timeout = 1;
         __threadfence();
@@ -1020,13 +1021,13 @@ __device__ __forceinline__ void form_theta(CtaScalars *sc, double2 *X, const dou
                     if (!trans) {
                         const int r = 2 * a + s0, j = 2 * (d - idx0) + s1;
                         const int slot = j >= w, jj = j - slot * w;
-                        X[(size_t)(slot * wmax + jj) * rpad + r] = m;
+                        if constexpr (WRITE_X) X[(size_t)(slot * wmax + jj) * rpad + r] = m;
                         x0[(size_t)r * C + s1 * cr + d] = m;
                     } else {
                         const int r = s1 * cr + d, j = 2 * (a - idx0) + s0;
                         const int slot = j >= w, jj = j - slot * w;
                         const double2 mc = c_conj(m);
-                        X[(size_t)(slot * wmax + jj) * rpad + r] = mc;
+                        if constexpr (WRITE_X) X[(size_t)(slot * wmax + jj) * rpad + r] = mc;
                         x0[(size_t)r * C + 2 * a + s0] = mc;
                     }
                 }
@@ -1687,7 +1688,7 @@ __global__ void theta_clear_kernel(const mpsb_pair *pairs, int npairs, int32_t *
 }
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kThetaThreads, 1) theta2q_kernel(ThetaParams p) {
+__global__ void __launch_bounds__(kThetaThreads, 2) theta2q_kernel(ThetaParams p) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     const int pi = blockIdx.x >> 1, half = blockIdx.x & 1, tid = threadIdx.x;
     CtaScalars *sc = reinterpret_cast<CtaScalars *>(smem_raw);
@@ -1721,8 +1722,8 @@ __global__ void __launch_bounds__(kThetaThreads, 1) theta2q_kernel(ThetaParams p
     const double2 *A = reinterpret_cast<const double2 *>(ch.sites + (size_t)i * ch.slot_elems);
     const double2 *B = reinterpret_cast<const double2 *>(ch.sites + (size_t)(i + 1) * ch.slot_elems);
     double2 *x0 = p.theta + (size_t)pr.out * (size_t)(2 * p.chi_cap) * (size_t)(2 * p.chi_cap);
-    form_theta<kThetaThreads, MIXED, false>(sc, X, A, B, cl, cm, cr, false, idx0, nidx, C, w, p.wmax, p.rpad, x0,
-                                            tid);
+    form_theta<kThetaThreads, MIXED, false, false>(sc, X, A, B, cl, cm, cr, false, idx0, nidx, C, w, p.wmax,
+                                                   p.rpad, x0, tid);
     __syncthreads();
     if (tid == 0) {
         const int flags = (sc->nonfinite ? MPSB_ST_NONFINITE : 0) | (sc->timeout ? MPSB_ST_TIMEOUT : 0);
@@ -1746,13 +1747,19 @@ int launch_theta2q(int precision, const mpsb_chain *chains, const mpsb_pair *pai
     // the same contraction as the update of this precision and cap
     bool mixed = precision != MPSB_FP64;
     if (precision == MPSB_MIXED_TF32X3 && rpl <= 2) mixed = false;
-    size_t smem = 384 + (size_t)2 * p.wmax * p.rpad * sizeof(double2);
+    // theta goes straight to global memory: shared memory holds the scalars
+    // and, for the tensor-core form, the operand staging area
+    size_t smem = 384;
     if (mixed) {
-        smem = upd_smem_bytes_mixed(p.wmax, p.rpad, chi_cap);
-        // at most four resident CTAs per SM, so that their TMEM (<= 128
-        // columns each at chi_cap <= 32; 256 above, where the shared memory
-        // allows one CTA per SM) always fits in the SM's 512 columns
-        if (smem < 57344) smem = 57344;
+        const size_t kpad = (size_t)((chi_cap + 7) & ~7);
+        const size_t npad = (size_t)max(16, ((2 * p.wmax) + 15) & ~15);
+        const size_t mt = p.rpad > 64 ? 128 : 64;
+        smem = 384 + 2 * mt * kpad * 4 + 2 * npad * kpad * 4;
+        // resident CTAs per SM times their TMEM columns (3 npad rounded up
+        // to a power of two: <= 128 at chi_cap <= 32, <= 256 above) must fit
+        // the SM's 512 columns: at most four, resp. two CTAs per SM
+        const size_t floor_bytes = chi_cap <= 32 ? 57344 : 80 * 1024;
+        if (smem < floor_bytes) smem = floor_bytes;
     }
     theta_clear_kernel<<<(npairs + 255) / 256, 256, 0, stream>>>(pairs, npairs, status);
     int rc = check_launch("theta_clear_kernel");
