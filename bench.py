@@ -696,7 +696,8 @@ def run_ours(args) -> None:
         trunc = np.concatenate([pb.trunc.cpu().numpy() for pb in pbs])  # discarded weight per update
         return {"batch": batch, "value": world * n_upd * args.steps / total_s, "total_s": total_s,
                 "flops": flops, "hbm": hbm, "kern_s": kern_s, "clocks": clk,
-                "achieved_tf": flops / kern_s / 1e12, "trunc": trunc}
+                "achieved_tf": flops / kern_s / 1e12, "trunc": trunc,
+                "layer_ms": [round(float(v) / args.steps, 4) for v in layer_ms]}
 
     # per-layer launches (one launch per layer), both forms: the reference point and the state checks
     main = measure(precision, timed=False)
@@ -747,6 +748,7 @@ def run_ours(args) -> None:
     mixed_v, fp64_v = (value, fother["value"]) if precision == "mixed" else (fother["value"], value)
     flops, hbm, kern_s, achieved_tf, clk = main["flops"], main["hbm"], fmain["kern_s"], fmain["achieved_tf"], fmain["clocks"]
     flow = {"per_layer_launches": {precision: round(main["value"], 3), other_prec: round(other["value"], 3)},
+            f"{precision}_ms_per_layer_launch": main["layer_ms"],
             "one_dataflow_launch": {precision: round(value, 3), other_prec: round(fother["value"], 3)},
             f"{precision}_bitwise_equal": fmain["bitwise_equal_to_per_layer"],
             f"{other_prec}_bitwise_equal": fother["bitwise_equal_to_per_layer"],
