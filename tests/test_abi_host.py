@@ -62,6 +62,21 @@ def test_argument_errors_need_no_device():
     assert rc == -3
     with pytest.raises(_lib.MPSBError, match="EINVAL"):
         _lib.check(-1, "probe")
+    # contraction only: same argument rules, checked before any device query
+    p = C.c_void_p(256)
+    assert lib.mpsb_contract2q_batch(None, None, 0, None, 0, 8, None, None, None) == 0
+    rc = lib.mpsb_contract2q_batch(p, p, -2, p, 0, 8, p, p, None)
+    assert rc == -1 and b"npairs" in lib.mpsb_last_error()
+    rc = lib.mpsb_contract2q_batch(p, p, 1, p, 0, 8, None, p, None)
+    assert rc == -1 and b"theta" in lib.mpsb_last_error()
+    rc = lib.mpsb_contract2q_batch(p, p, 1, p, 0, 65, p, p, None)
+    assert rc == -1 and b"chi_cap" in lib.mpsb_last_error()
+    rc = lib.mpsb_contract2q_batch(p, p, 1, p, 3, 8, p, p, None)
+    assert rc == -1 and b"precision" in lib.mpsb_last_error()
+    # the TF32 probe bounds its MMA chain
+    assert lib.mpsb_tf32_probe(0, 1, p, None) == -1
+    assert lib.mpsb_tf32_probe(65537, 1, p, None) == -1
+    assert lib.mpsb_tf32_probe(1024, 0, p, None) == -1
 
 
 def test_keep_limit_and_status_names():

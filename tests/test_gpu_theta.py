@@ -191,3 +191,45 @@ def test_tf32_probe_counts_and_rate():
     assert tflops > 100.0, tflops  # a dense tensor-core rate, not a fallback
     with pytest.raises(RuntimeError):
         _lib.check(lib.mpsb_tf32_probe(1 << 20, sms, sink.data_ptr(), stream.cuda_stream), "tf32 probe")
+
+
+def test_pairs_of_many_chains_and_graph_replay():
+    """Pairs of uneven chains in one launch; the launch captured in a CUDA graph
+    and replayed gives the same thetas bit for bit."""
+    from fpga_mps_simulator_b200 import MPSBatch
+    from fpga_mps_simulator_b200.circuits import brickwall_layers
+    ns = [6, 11, 9]
+    b = MPSBatch(ns, [8, 16, 4], [1e-12] * 3)
+    refs = [OracleMPS(n, chi, 1e-12) for n, chi in zip(ns, [8, 16, 4])]
+    for c, n in enumerate(ns):
+        for L in brickwall_layers(n, 5, 20 + c):
+            b.apply_layer(np.full(len(L.sites), c, np.int32), L.sites, L.gates)
+            for i, g in zip(L.sites, L.gates):
+                refs[c].apply_adjacent_2q(int(i), g)
+    rng = np.random.default_rng(9)
+    chain_idx = np.array([0, 2, 1, 1, 0, 2], np.int32)
+    sites = np.array([2, 0, 5, 9, 4, 7], np.int32)
+    gates = np.stack([_haar(rng) for _ in sites])
+    tb = b.make_thetas(chain_idx, sites, gates)
+    b.run_thetas(tb)
+    torch.cuda.synchronize()
+    assert not tb.status.any().item()
+    first = tb.theta.clone()
+    for k, (c, i) in enumerate(zip(chain_idx, sites)):
+        want = _oracle_theta(refs[c].sites[i], refs[c].sites[i + 1], gates[k])
+        got = tb.matrices()[k]
+        s_got, s_want = np.linalg.svd(got, compute_uv=False), np.linalg.svd(want, compute_uv=False)
+        np.testing.assert_allclose(s_got, s_want, rtol=0, atol=1e-10 * s_want[0])
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    tb.theta.zero_()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(g, stream=s):
+        b.run_thetas(tb, stream=s)
+    for _ in range(2):
+        tb.theta.zero_()
+        g.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(tb.theta, first)
+    del g
