@@ -769,7 +769,10 @@ __device__ __forceinline__ void apply_panel(double2 (&Y)[4][RPL], const double2 
 // costing ~2.3 sweeps there.  A 2e-2 gate was 2 % faster than 5e-3 on the
 // ansatz (fewer slow unpreconditioned pairs in each wave) and within noise
 // on brickwork.
-constexpr double kPrecondSpread = 2e-2;
+#ifndef MPSB_PRECOND_SPREAD
+#define MPSB_PRECOND_SPREAD 2e-2
+#endif
+constexpr double kPrecondSpread = MPSB_PRECOND_SPREAD;
 
 // Decide whether to precondition (both CTAs reach the same answer from the
 // same keys).  If so, sort the columns by decreasing norm (ties by column
@@ -1689,7 +1692,7 @@ __global__ void theta_clear_kernel(const mpsb_pair *pairs, int npairs, int32_t *
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kThetaThreads, 2) theta2q_kernel(ThetaParams p) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int pi = blockIdx.x >> 1, half = blockIdx.x & 1, tid = threadIdx.x;
     CtaScalars *sc = reinterpret_cast<CtaScalars *>(smem_raw);
     double2 *X = reinterpret_cast<double2 *>(smem_raw + 384);
