@@ -769,6 +769,12 @@ __device__ __forceinline__ void apply_panel(double2 (&Y)[4][RPL], const double2 
 // costing ~2.3 sweeps there.  A 2e-2 gate was 2 % faster than 5e-3 on the
 // ansatz (fewer slow unpreconditioned pairs in each wave) and within noise
 // on brickwork.
+// Kept vectors per pass of the split's GEMM (accumulators per thread):
+// measured 8 against 4 (config 2 -2 %, gradient step equal) and 16 (config 2
+// -0.5 %, the chi = 32 gradient step +17 %: more spills at 168 registers).
+#ifndef MPSB_SPLIT_VECS
+#define MPSB_SPLIT_VECS 8
+#endif
 #ifndef MPSB_PRECOND_SPREAD
 #define MPSB_PRECOND_SPREAD 2e-2
 #endif
@@ -1260,6 +1266,8 @@ __device__ __forceinline__ void update_pair(const Upd2Params &p, const int pi, c
         const int slot = j >= w, jj = j - slot * w;
         return X + (size_t)(slot * wmax + jj) * rpad;
     };
+    // kept vectors per pass of the other side's GEMM (its accumulators per thread)
+    constexpr int kSplitVecs = MPSB_SPLIT_VECS;
     if (precond) {
         // The converged columns z_j (C rows) are X's right singular vectors
         // times S with rows in sorted order (row i = column perm[i] of X0):
@@ -1284,12 +1292,12 @@ __device__ __forceinline__ void update_pair(const Upd2Params &p, const int pi, c
         const int grp = tid / kRows;
         for (int r = tid - grp * kRows; r < R; r += kRows) {
             const double2 *xr = x0 + (size_t)r * C;
-            for (int base = grp * 8; base < nk; base += 8 * kGroups) {
-                const int nb = min(8, nk - base);
-                const double2 *cpk[8];
-                double2 acc[8];
+            for (int base = grp * kSplitVecs; base < nk; base += kSplitVecs * kGroups) {
+                const int nb = min(kSplitVecs, nk - base);
+                const double2 *cpk[kSplitVecs];
+                double2 acc[kSplitVecs];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
+                for (int q = 0; q < kSplitVecs; ++q) {
                     cpk[q] = colp(klist[base + (q < nb ? q : 0)]);
                     acc[q] = make_double2(0.0, 0.0);
                 }
@@ -1297,10 +1305,10 @@ __device__ __forceinline__ void update_pair(const Upd2Params &p, const int pi, c
                     const int col = perm[c];
                     const double2 xv = (col >= 0 && col < C) ? __ldcg(xr + col) : make_double2(0.0, 0.0);
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) acc[q] = c_fma(xv, cpk[q][c], acc[q]);
+                    for (int q = 0; q < kSplitVecs; ++q) acc[q] = c_fma(xv, cpk[q][c], acc[q]);
                 }
 #pragma unroll
-                for (int q = 0; q < 8; ++q) {
+                for (int q = 0; q < kSplitVecs; ++q) {
                     if (q < nb) {
                         const int rho = rank[klist[base + q]];
                         const double sg = Ssorted[rho];
@@ -1333,22 +1341,22 @@ __device__ __forceinline__ void update_pair(const Upd2Params &p, const int pi, c
             constexpr int kGroups = NT / kCols;
             const int grp = tid / kCols;
             for (int col = tid - grp * kCols; col < C; col += kCols) {
-                for (int base = grp * 8; base < nk; base += 8 * kGroups) {
-                    const int nb = min(8, nk - base);
-                    const double2 *cpk[8];
-                    double2 acc[8];
+                for (int base = grp * kSplitVecs; base < nk; base += kSplitVecs * kGroups) {
+                    const int nb = min(kSplitVecs, nk - base);
+                    const double2 *cpk[kSplitVecs];
+                    double2 acc[kSplitVecs];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
+                    for (int q = 0; q < kSplitVecs; ++q) {
                         cpk[q] = colp(klist[base + (q < nb ? q : 0)]);
                         acc[q] = make_double2(0.0, 0.0);
                     }
                     for (int r = 0; r < R; ++r) {
                         const double2 xv = __ldcg(x0 + (size_t)r * C + col);
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) acc[q] = c_cfma(cpk[q][r], xv, acc[q]);
+                        for (int q = 0; q < kSplitVecs; ++q) acc[q] = c_cfma(cpk[q][r], xv, acc[q]);
                     }
 #pragma unroll
-                    for (int q = 0; q < 8; ++q) {
+                    for (int q = 0; q < kSplitVecs; ++q) {
                         if (q < nb) {
                             const int rho = rank[klist[base + q]];
                             const double sg = Ssorted[rho];
