@@ -564,7 +564,11 @@ def cpu_baseline_sample(workers: int):
         pool.close()
         pool.join()
     one = single_process_default_threads(CHI, 40, SEED)
-    return {"value": round(r["updates_per_s"], 3), "unit": UNIT, "cores": workers, "kind": "port",
+    # untimed: the oracle's own final state of the benchmark circuit (seed SEED, as rank 0's),
+    # the FP64 reference the device forms' infidelity is reported against
+    ref = run_parallel(N_SITES, DEPTH, CHI, CUTOFF, 1, reps=1, seed=SEED, keep_first=True)
+    return {"_final": (ref["final_sites"], ref["final_norm_log"]),
+            "value": round(r["updates_per_s"], 3), "unit": UNIT, "cores": workers, "kind": "port",
             "sample": (f"{workers} single-BLAS-thread processes, each one full n={N_SITES} depth-{DEPTH} "
                        f"chi={CHI} circuit ({r['updates']} updates, {r['wall_s']:.1f} s wall); oracle "
                        "restatement of mps_core.py with scipy gesdd"),
@@ -767,11 +771,31 @@ def run_ours(args) -> None:
     zterms = [(i, zop, None) for i in range(N_SITES)]
     z_main = main["batch"].expect_terms(zterms)[0]
     z_other = other["batch"].expect_terms(zterms)[0]
+    # both forms against the oracle's final state of the same circuit (the FP64 reference of
+    # the metric), overlaps taken on the device
+    vs_oracle = None
+    if cpu is not None and cpu.get("_final") is not None:
+        sites_ref, nl_ref = cpu.pop("_final")
+        rb = MPSBatch([N_SITES], [CHI], [CUTOFF], precision="fp64", device=dev)
+        for k, t in enumerate(sites_ref):
+            rb.set_site(0, k, t)
+        rb.norm_logs.fill_(nl_ref)
+        rr, lrr = overlap(rb, 0, rb, 0)
+        vs_oracle = {}
+        for name, res in ((precision, main), (other_prec, other)):
+            xb, lxb = overlap(res["batch"], 0, rb, 0)
+            xx, lxx = overlap(res["batch"], 0, res["batch"], 0)
+            vs_oracle[name] = 1.0 - abs(xb) ** 2 / (xx.real * rr.real) * math.exp(2 * lxb - lxx - lrr)
+        vs_oracle["note"] = ("final state of each device form against the oracle's (mps_core semantics, "
+                             "scipy gesdd, FP64) final state of the same circuit")
+        del rb
     tr_m, tr_o = main["trunc"], other["trunc"]
     form_errors = {"discarded_weight_per_update": {f"{precision}_mean": float(tr_m.mean()),
                                                    f"{other_prec}_mean": float(tr_o.mean()),
                                                    "max_abs_diff": float(np.max(np.abs(tr_m - tr_o)))},
                    "z_expectation_max_abs_diff": float(np.max(np.abs(z_main - z_other)))}
+    if vs_oracle is not None:
+        form_errors["infidelity_vs_oracle"] = vs_oracle
 
     # ---- mixed vs FP64 state infidelity as the circuit deepens (untimed replay)
     by_depth = {}

@@ -34,8 +34,11 @@ def _circuit(n: int, depth: int, seed: int) -> List[Tuple[int, np.ndarray]]:
     return out
 
 
-def _worker(args) -> Tuple[int, float]:
-    n, depth, chi, cutoff, seed, reps = args
+def _worker(args) -> tuple:
+    """(updates, seconds) -- plus the final sites and norm_log when `keep` is set,
+    so the run can serve as the FP64 reference the device states are checked
+    against."""
+    n, depth, chi, cutoff, seed, reps, keep = args
     try:
         from threadpoolctl import threadpool_limits
         limiter = threadpool_limits(1)
@@ -58,6 +61,8 @@ def _worker(args) -> Tuple[int, float]:
         count += len(gates)
     dt = time.perf_counter() - t0
     del limiter
+    if keep:
+        return count, dt, [np.ascontiguousarray(a) for a in st.sites], float(st.norm_log)
     return count, dt
 
 
@@ -69,22 +74,29 @@ def usable_cores() -> int:
 
 
 def run_parallel(n: int, depth: int, chi: int, cutoff: float, workers: int, reps: int = 1,
-                 seed: int = 0, pool=None) -> Dict[str, float]:
-    """Aggregate updates/s of `workers` single-threaded processes, each running `reps` circuits."""
+                 seed: int = 0, pool=None, keep_first: bool = False) -> Dict[str, float]:
+    """Aggregate updates/s of `workers` single-threaded processes, each running `reps` circuits.
+
+    keep_first: also return worker 0's final state (the circuit of `seed`) as
+    `final_sites` / `final_norm_log`."""
     own = pool is None
     if own:
         pool = _single_thread_pool(workers)
     try:
         t0 = time.perf_counter()
-        res = pool.map(_worker, [(n, depth, chi, cutoff, seed + w, reps) for w in range(workers)])
+        res = pool.map(_worker, [(n, depth, chi, cutoff, seed + w, reps, keep_first and w == 0)
+                                 for w in range(workers)])
         wall = time.perf_counter() - t0
     finally:
         if own:
             pool.close()
             pool.join()
     updates = sum(r[0] for r in res)
-    return {"updates": updates, "wall_s": wall, "updates_per_s": updates / wall,
-            "per_worker_s": float(np.mean([r[1] for r in res])), "workers": workers}
+    out = {"updates": updates, "wall_s": wall, "updates_per_s": updates / wall,
+           "per_worker_s": float(np.mean([r[1] for r in res])), "workers": workers}
+    if keep_first:
+        out["final_sites"], out["final_norm_log"] = res[0][2], res[0][3]
+    return out
 
 
 _SINGLE_THREAD_ENV = ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS", "BLIS_NUM_THREADS")
