@@ -129,8 +129,13 @@ __device__ __forceinline__ uint32_t core_off(int row, int k, int kc) {
 // The accumulator of an M = 128 MMA holds row m in TMEM lane m; that of an
 // M = 64 MMA (one CTA) holds row m = m0 + 16 m1 (m0 < 16, m1 < 4) in lane
 // m0 + 32 m1, the first half of each warp's 32-lane quarter.
+// corr: the correction products hi*lo and lo*hi accumulate in a second bank
+// of accumulators 3 npad columns on (M = 128 tiles), so the fp32 rounding of
+// the large hi*hi sum does not also swallow the low bits of the corrections;
+// the two banks are added in FP64 on read-back.
 struct TcShape {
     int mvalid, nvalid, kpad, npad, mt;
+    bool corr;
 };
 __device__ __forceinline__ int tmem_lane_of_row(int m, int mt) { return mt == 128 ? m : (m & 15) + 32 * (m >> 4); }
 
@@ -213,11 +218,13 @@ __device__ __forceinline__ void issue_product(unsigned char *buf, uint32_t tmem,
     const uint32_t sbo = static_cast<uint32_t>(kc) * 128u;
     const uint32_t idesc = tc::make_idesc_tf32(sh.mt, sh.npad);
     const uint32_t d = tmem + static_cast<uint32_t>(dcol);
+    const uint32_t dc = sh.corr ? d + static_cast<uint32_t>(3 * sh.npad) : d;  // correction bank
     for (int s = 0; s < (sh.kpad >> 3); ++s) {
         const uint32_t step = static_cast<uint32_t>(s) * 256u;  // two 16-byte K chunks per K = 8 step
         tc::mma_tf32(d, tc::make_desc(ahi + step, 128, sbo), tc::make_desc(bhi + step, 128, sbo), idesc, s > 0);
-        tc::mma_tf32(d, tc::make_desc(ahi + step, 128, sbo), tc::make_desc(blo + step, 128, sbo), idesc, 1);
-        tc::mma_tf32(d, tc::make_desc(alo + step, 128, sbo), tc::make_desc(bhi + step, 128, sbo), idesc, 1);
+        tc::mma_tf32(dc, tc::make_desc(ahi + step, 128, sbo), tc::make_desc(blo + step, 128, sbo), idesc,
+                     (sh.corr && s == 0) ? 0u : 1u);
+        tc::mma_tf32(dc, tc::make_desc(alo + step, 128, sbo), tc::make_desc(bhi + step, 128, sbo), idesc, 1);
     }
 }
 
@@ -242,16 +249,34 @@ __device__ void read_theta(uint32_t tmem, const TcShape &sh, const double2 *g, b
     for (int ch = warp >> 2; ch < nchunks; ch += kChunkStride) {
         const uint32_t base = tmem + (static_cast<uint32_t>(32 * qr) << 16) + static_cast<uint32_t>(16 * ch);
         float p1[16], p2[16], p3[16];
+        double d1[16], d2[16], d3[16];
         tc::tmem_ld16(base, p1);
         tc::tmem_ld16(base + static_cast<uint32_t>(sh.npad), p2);
         tc::tmem_ld16(base + static_cast<uint32_t>(2 * sh.npad), p3);
 #pragma unroll
+        for (int q = 0; q < 16; ++q) {
+            d1[q] = p1[q];
+            d2[q] = p2[q];
+            d3[q] = p3[q];
+        }
+        if (sh.corr) {  // add the correction bank in FP64
+            tc::tmem_ld16(base + static_cast<uint32_t>(3 * sh.npad), p1);
+            tc::tmem_ld16(base + static_cast<uint32_t>(4 * sh.npad), p2);
+            tc::tmem_ld16(base + static_cast<uint32_t>(5 * sh.npad), p3);
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                d1[q] += p1[q];
+                d2[q] += p2[q];
+                d3[q] += p3[q];
+            }
+        }
+#pragma unroll
         for (int jj = 0; jj < 8; ++jj) {
             // own row m: columns n = 16 ch + 2 jj + {0, 1}
-            const double o0r = (double)p1[2 * jj] - (double)p2[2 * jj];
-            const double o0i = (double)p3[2 * jj] - (double)p1[2 * jj] - (double)p2[2 * jj];
-            const double o1r = (double)p1[2 * jj + 1] - (double)p2[2 * jj + 1];
-            const double o1i = (double)p3[2 * jj + 1] - (double)p1[2 * jj + 1] - (double)p2[2 * jj + 1];
+            const double o0r = d1[2 * jj] - d2[2 * jj];
+            const double o0i = d3[2 * jj] - d1[2 * jj] - d2[2 * jj];
+            const double o1r = d1[2 * jj + 1] - d2[2 * jj + 1];
+            const double o1i = d3[2 * jj + 1] - d1[2 * jj + 1] - d2[2 * jj + 1];
             const double q0r = __shfl_xor_sync(0xffffffffu, o0r, 1), q0i = __shfl_xor_sync(0xffffffffu, o0i, 1);
             const double q1r = __shfl_xor_sync(0xffffffffu, o1r, 1), q1i = __shfl_xor_sync(0xffffffffu, o1i, 1);
             const int col = 8 * ch + jj;  // index within the CTA's share (dd or aa)
@@ -315,8 +340,11 @@ __device__ bool contract_mixed(unsigned char *opbuf, uint64_t *mbar, uint32_t *t
     sh.npad = max(16, (sh.nvalid + 15) & ~15);
     sh.kpad = (cm + 7) & ~7;
     sh.mt = rpad > 64 ? 128 : 64;  // rows of a column: 128 above chi_cap 32, at most 64 below
-    const int need = 3 * sh.npad;
-    const uint32_t ncols = need <= 32 ? 32u : need <= 64 ? 64u : need <= 128 ? 128u : 256u;
+    // (the 64-row tiles run three CTAs per SM, whose TMEM must fit together:
+    // one bank there)
+    sh.corr = sh.mt == 128;
+    const int need = (sh.corr ? 6 : 3) * sh.npad;
+    const uint32_t ncols = need <= 32 ? 32u : need <= 64 ? 64u : need <= 128 ? 128u : need <= 256 ? 256u : 512u;
     if ((tid >> 5) == 0) tc::tmem_alloc(tmem_slot, ncols);
     if (tid == 0) {
         tc::mbar_init(mbar, 1);

@@ -1766,10 +1766,10 @@ int launch_theta2q(int precision, const mpsb_chain *chains, const mpsb_pair *pai
         const size_t npad = (size_t)max(16, ((2 * p.wmax) + 15) & ~15);
         const size_t mt = p.rpad > 64 ? 128 : 64;
         smem = 384 + 2 * mt * kpad * 4 + 2 * npad * kpad * 4;
-        // resident CTAs per SM times their TMEM columns (3 npad rounded up
-        // to a power of two: <= 128 at chi_cap <= 32, <= 256 above) must fit
-        // the SM's 512 columns: at most four, resp. two CTAs per SM
-        const size_t floor_bytes = chi_cap <= 32 ? 57344 : 80 * 1024;
+        // resident CTAs per SM times their TMEM columns must fit the SM's
+        // 512: at chi_cap <= 32 (3 npad <= 96 -> 128 columns) at most four
+        // CTAs per SM, above it (two banks, 6 npad <= 384 -> 512) one
+        const size_t floor_bytes = chi_cap <= 32 ? 57344 : 120 * 1024;
         if (smem < floor_bytes) smem = floor_bytes;
     }
     theta_clear_kernel<<<(npairs + 255) / 256, 256, 0, stream>>>(pairs, npairs, status);
