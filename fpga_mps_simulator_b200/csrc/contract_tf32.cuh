@@ -3,7 +3,8 @@
 // P1 = Re A Re B, P2 = Im A Im B, P3 = (Re A + Im A)(Re B + Im B); then
 // Re T = P1 - P2, Im T = P3 - P1 - P2), each real GEMM in split-precision
 // 3xTF32 (a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi, FP32 accumulation in
-// TMEM).  The 4x4 gate is then mixed in FP64 while reading the accumulators
+// TMEM; at M = 128 the two correction terms in an accumulator bank of their
+// own, added in FP64 on read-back).  The 4x4 gate is then mixed in FP64 while reading the accumulators
 // back, and the result lands in the Jacobi slots exactly like the FP64 path.
 //
 // Included by update2q.cu only.  One CTA issues its own cta_group::1 MMAs
