@@ -25,6 +25,7 @@
 //   over full circuits).
 #include "mpsb_common.cuh"
 #include "contract_tf32.cuh"
+#include "cta_gemm.cuh"
 
 #include <cstdio>
 #include <cstdlib>
@@ -1287,36 +1288,58 @@ __device__ __forceinline__ void update_pair(const Upd2Params &p, const int pi, c
                 Aout[(size_t)col * K + rho] = c_scale(v, f);
         }
         const double2 *x0 = x0pair;
-        constexpr int kRows = NT < 128 ? NT : 128;  // threads per row group
-        constexpr int kGroups = NT / kRows;
-        const int grp = tid / kRows;
-        for (int r = tid - grp * kRows; r < R; r += kRows) {
-            const double2 *xr = x0 + (size_t)r * C;
-            for (int base = grp * kSplitVecs; base < nk; base += kSplitVecs * kGroups) {
-                const int nb = min(kSplitVecs, nk - base);
-                const double2 *cpk[kSplitVecs];
-                double2 acc[kSplitVecs];
-#pragma unroll
-                for (int q = 0; q < kSplitVecs; ++q) {
-                    cpk[q] = colp(klist[base + (q < nb ? q : 0)]);
-                    acc[q] = make_double2(0.0, 0.0);
-                }
-                for (int c = 0; c < C; ++c) {
+        if constexpr (RPL == 4 && NT == kCtaGemmThreads) {
+            // U S^2 = X0 P z_k as one CTA GEMM on FP64 MMAs (R x nk x C), its
+            // operand tiles in the staging block
+            cta_cgemm<true, false>(
+                R, nk, C,
+                [&](int r, int c) {
                     const int col = perm[c];
-                    const double2 xv = (col >= 0 && col < C) ? __ldcg(xr + col) : make_double2(0.0, 0.0);
-#pragma unroll
-                    for (int q = 0; q < kSplitVecs; ++q) acc[q] = c_fma(xv, cpk[q][c], acc[q]);
-                }
-#pragma unroll
-                for (int q = 0; q < kSplitVecs; ++q) {
-                    if (q < nb) {
-                        const int rho = rank[klist[base + q]];
-                        const double sg = Ssorted[rho];
-                        const double f = sg > 0.0 ? sqrt(sg / div) / (sg * sg) : 0.0;
-                        if (!trans)
-                            Aout[(size_t)r * K + rho] = c_scale(acc[q], f);
-                        else
-                            Bout[(size_t)rho * R + r] = c_scale(c_conj(acc[q]), f);
+                    return (col >= 0 && col < C) ? __ldcg(x0 + (size_t)r * C + col) : make_double2(0.0, 0.0);
+                },
+                [&](int c, int kk) { return colp(klist[kk])[c]; },
+                [&](int r, int kk, double2 v) {
+                    const int rho = rank[klist[kk]];
+                    const double sg = Ssorted[rho];
+                    const double f = sg > 0.0 ? sqrt(sg / div) / (sg * sg) : 0.0;
+                    if (!trans)
+                        Aout[(size_t)r * K + rho] = c_scale(v, f);
+                    else
+                        Bout[(size_t)rho * R + r] = c_scale(c_conj(v), f);
+                },
+                *reinterpret_cast<GemmSmem *>(stage));
+        } else {
+            constexpr int kRows = NT < 128 ? NT : 128;  // threads per row group
+            constexpr int kGroups = NT / kRows;
+            const int grp = tid / kRows;
+            for (int r = tid - grp * kRows; r < R; r += kRows) {
+                const double2 *xr = x0 + (size_t)r * C;
+                for (int base = grp * kSplitVecs; base < nk; base += kSplitVecs * kGroups) {
+                    const int nb = min(kSplitVecs, nk - base);
+                    const double2 *cpk[kSplitVecs];
+                    double2 acc[kSplitVecs];
+    #pragma unroll
+                    for (int q = 0; q < kSplitVecs; ++q) {
+                        cpk[q] = colp(klist[base + (q < nb ? q : 0)]);
+                        acc[q] = make_double2(0.0, 0.0);
+                    }
+                    for (int c = 0; c < C; ++c) {
+                        const int col = perm[c];
+                        const double2 xv = (col >= 0 && col < C) ? __ldcg(xr + col) : make_double2(0.0, 0.0);
+    #pragma unroll
+                        for (int q = 0; q < kSplitVecs; ++q) acc[q] = c_fma(xv, cpk[q][c], acc[q]);
+                    }
+    #pragma unroll
+                    for (int q = 0; q < kSplitVecs; ++q) {
+                        if (q < nb) {
+                            const int rho = rank[klist[base + q]];
+                            const double sg = Ssorted[rho];
+                            const double f = sg > 0.0 ? sqrt(sg / div) / (sg * sg) : 0.0;
+                            if (!trans)
+                                Aout[(size_t)r * K + rho] = c_scale(acc[q], f);
+                            else
+                                Bout[(size_t)rho * R + r] = c_scale(c_conj(acc[q]), f);
+                        }
                     }
                 }
             }
@@ -1335,7 +1358,26 @@ __device__ __forceinline__ void update_pair(const Upd2Params &p, const int pi, c
                 Bout[(size_t)rho * R + r] = c_scale(c_conj(v), f);
         }
         // other side: Y[rho, col] = sum_r conj(x_j[r]) X0[r, col]
-        {
+        if constexpr (RPL == 4 && NT == kCtaGemmThreads) {
+            // 128-row theta: one CTA GEMM on FP64 MMAs (nk x C x R), its
+            // operand tiles in the staging block, which the sweeps no longer need
+            // (the smallest staging block at 128 rows: chi_cap 33, 20 columns)
+            static_assert(sizeof(GemmSmem) <= 20 * 128 * sizeof(double2), "GEMM tiles exceed the staging block");
+            const double2 *x0 = x0pair;
+            cta_cgemm<true, true>(
+                nk, C, R, [&](int ii, int r) { return c_conj(colp(klist[ii])[r]); },
+                [&](int r, int col) { return __ldcg(x0 + (size_t)r * C + col); },
+                [&](int ii, int col, double2 v) {
+                    const int rho = rank[klist[ii]];
+                    const double sg = Ssorted[rho];
+                    const double f = sg > 0.0 ? sqrt(sg / div) / (sg * sg) : 0.0;
+                    if (!trans)
+                        Bout[(size_t)rho * C + col] = c_scale(v, f);
+                    else
+                        Aout[(size_t)col * K + rho] = c_scale(c_conj(v), f);
+                },
+                *reinterpret_cast<GemmSmem *>(stage));
+        } else {
             const double2 *x0 = x0pair;
             constexpr int kCols = NT < 128 ? NT : 128;  // threads per column group
             constexpr int kGroups = NT / kCols;
