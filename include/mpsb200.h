@@ -138,7 +138,9 @@ MPSB_API size_t mpsb_update2q_workspace_bytes(int npairs, int chi_cap);
  * 2-norm (norm_log += log norm when norm > 1e-15), sites i and i+1 replaced by
  * U sqrt(S) and sqrt(S) Vh in place, bonds[i+1] = keep.
  *   chains, pairs, gates: device.  chi_cap: largest bond of any chain touched.
- *   tol: Jacobi off-diagonal tolerance (<= 0 picks the form's default).
+ *   tol: Jacobi off-diagonal tolerance (<= 0 picks the form's default): a column
+ *        pair rotates when |x^H y|^2 > tol^2 |x|^2 |y|^2; the sweeps end after a
+ *        sweep in which no pair had |x^H y|^2 > 2 tol |x|^2 |y|^2.
  *   max_sweeps: Jacobi sweep bound (<= 0 picks 40).
  *   spectra (nullable): npairs_out x 128 doubles, full descending spectrum.
  *   kept, trunc (nullable): kept count and discarded weight dropped/total.
