@@ -93,7 +93,7 @@ struct PairRec {
 // rounded up to a multiple of 16 double2 (256 bytes).
 constexpr int kTapeMetaKeep = 128, kTapeMetaDiv = 129, kTapeMetaRows = 130, kTapeMetaCols = 131;
 constexpr int kTapeMetaSide = 132;
-constexpr int kTapeMetaSweeps = 133;  // Jacobi sweeps taken (the final one without rotations included)
+constexpr int kTapeMetaSweeps = 133;  // Jacobi sweeps taken (the final one, with no rotation above the stop bound, included)
 __host__ __device__ inline long long tape_stride(int chi_cap) {
     const long long q = (long long)(2 * chi_cap) * (2 * chi_cap);
     return (2 * q + 72 + 15) & ~15LL;

@@ -519,6 +519,85 @@ __device__ void cross_rounds(const Slots &S, int *stamp, int nq, int R0, int war
     store_quad<RPL>(S, 0, t, lane, P, p);
 }
 
+// One step's rounds with a single quad_cross call site: the round-robin
+// rounds inside each slot (step 0, after the inner pairs) and the cross
+// rounds between the slots run through the same loop body, and the slot-0
+// quad of a cross round is reloaded from shared memory every round instead of
+// staying in registers.  Same pairs, same order, same stamps as
+// internal_rounds + cross_rounds; four fewer inlined copies of the rotation
+// core, for the <= 64-row kernels, whose co-resident CTAs run different
+// phases and starve on instruction fetch.
+template <int RPL, int NT>
+__device__ void step_rounds_compact(const Slots &S, int *stamp, int nq, bool internal, int warp, int lane, JTol jt,
+                                    int &cnt, int &tmo) {
+    constexpr int kWarps = NT / 32;
+    if (internal) {
+        for (int t = 2 * warp; t < 2 * nq; t += 2 * kWarps) {
+            const int sa = t / nq, qa = t - sa * nq, sb = (t + 1) / nq, qb = (t + 1) - sb * nq;
+            double2 A[4][RPL], B[4][RPL];
+            double a[4], b[4];
+            load_quad<RPL>(S, sa, qa, lane, A, a);
+            load_quad<RPL>(S, sb, qb, lane, B, b);
+            cnt += quad_inner2<RPL>(A, a, B, b, lane, jt);
+            store_quad<RPL>(S, sa, qa, lane, A, a);
+            store_quad<RPL>(S, sb, qb, lane, B, b);
+            set_stamp(&stamp[sa * 8 + qa], 1, lane);
+            set_stamp(&stamp[sb * 8 + qb], 1, lane);
+        }
+    }
+    const int nq2 = nq + (nq & 1);
+    const int half = nq2 >> 1;
+    const int nrr = internal ? nq2 - 1 : 0;
+    const int R0 = internal ? nq2 : 0;
+#pragma unroll 1
+    for (int k = 0; k < nrr + nq; ++k) {
+        const bool rr = k < nrr;
+        const int ntask = rr ? 2 * half : nq;
+#pragma unroll 1
+        for (int t = warp; t < ntask; t += kWarps) {
+            int ia, ib, wa, wb, setb;
+            bool seta = true;
+            if (rr) {
+                const int slot = t / half, kk = t - slot * half;
+                const int u = rr_elem(kk, k, nq2), v = rr_elem(nq2 - 1 - kk, k, nq2);
+                if (!(u < nq && v < nq)) {  // a quad drawn against the dummy only advances its stamp
+                    const int real = u < nq ? u : v;
+                    if (real < nq) {
+                        wait_stamp(&stamp[slot * 8 + real], k + 1, lane, tmo);
+                        set_stamp(&stamp[slot * 8 + real], k + 2, lane);
+                    }
+                    continue;
+                }
+                ia = slot * 8 + u;
+                ib = slot * 8 + v;
+                wa = wb = k + 1;
+                setb = k + 2;
+            } else {
+                const int r = k - nrr;
+                int v = t + r;
+                if (v >= nq) v -= nq;
+                ia = t;  // slot 0: private to this warp for the whole step
+                ib = 8 + v;
+                wa = R0;
+                wb = R0 + r;
+                setb = R0 + r + 1;
+                seta = false;
+            }
+            wait_stamp(&stamp[ia], wa, lane, tmo);
+            wait_stamp(&stamp[ib], wb, lane, tmo);
+            double2 P[4][RPL], Q[4][RPL];
+            double p[4], q[4];
+            load_quad<RPL>(S, ia >> 3, ia & 7, lane, P, p);
+            load_quad<RPL>(S, ib >> 3, ib & 7, lane, Q, q);
+            cnt += quad_cross<RPL>(P, p, Q, q, lane, jt);
+            store_quad<RPL>(S, ia >> 3, ia & 7, lane, P, p);
+            store_quad<RPL>(S, ib >> 3, ib & 7, lane, Q, q);
+            if (seta) set_stamp(&stamp[ia], setb, lane);
+            set_stamp(&stamp[ib], setb, lane);
+        }
+    }
+}
+
 template <int RPL, int NT>
 __device__ void recompute_norms(const Slots &S, int w, int warp, int lane) {
     constexpr int kUpdWarps = NT / 32;
@@ -1172,9 +1251,15 @@ __device__ __forceinline__ void update_pair(const Upd2Params &p, const int pi, c
         for (int step = 0; step < 3; ++step) {
             if (tid < 16) sc->stamp[tid] = 0;
             __syncthreads();
-            int R0 = 0;
-            if (step == 0) R0 = internal_rounds<RPL, NT>(S, sc->stamp, w >> 2, warp, lane, JTol{p.tol2, p.stop2}, cnt, tmo);
-            cross_rounds<RPL, NT>(S, sc->stamp, w >> 2, R0, warp, lane, JTol{p.tol2, p.stop2}, cnt, tmo);
+            if constexpr (RPL < 4) {
+                step_rounds_compact<RPL, NT>(S, sc->stamp, w >> 2, step == 0, warp, lane, JTol{p.tol2, p.stop2}, cnt,
+                                             tmo);
+            } else {
+                int R0 = 0;
+                if (step == 0)
+                    R0 = internal_rounds<RPL, NT>(S, sc->stamp, w >> 2, warp, lane, JTol{p.tol2, p.stop2}, cnt, tmo);
+                cross_rounds<RPL, NT>(S, sc->stamp, w >> 2, R0, warp, lane, JTol{p.tol2, p.stop2}, cnt, tmo);
+            }
             __syncthreads();
             if (step == 2 && cnt) atomicAdd(&sc->nrot[sb], cnt);
             exchange_slots<NT>(cluster, S, stage, stage_nrm, crank, parity, w, tid);
