@@ -436,51 +436,83 @@ def large_leg(dev, precision: str = "fp64"):
 
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples taken while the timed region runs."""
+    """nvidia-smi clock / throttle-reason samples taken while the timed region runs.
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    nvidia-smi takes a few hundred ms to produce its first sample and may hold
+    its output until it exits, so it is started ahead of the timed region
+    (begin() marks the region's start, stop() its end) and every sample
+    carries its own timestamp: the samples inside the region are kept, and
+    when the region is shorter than the sampling interval, the nearest sample
+    on each side of it.
+    """
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 50
 
     def __init__(self, gpu_id: str):
+        import datetime
+        self._now = datetime.datetime.now
         self.path = tempfile.mktemp(suffix=".csv")
         self.proc = None
+        self.t0 = self.t1 = None
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", gpu_id, f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.8)  # first samples under way before the region starts
         except Exception:
             self.proc = None
 
+    def begin(self) -> None:
+        self.t0 = self._now()
+
     def stop(self):
+        import datetime
         if self.proc is None:
             return None
+        self.t1 = self._now()
+        time.sleep(2.0 * self.PERIOD_MS / 1000.0)  # one more sample after the region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
         self.fh.close()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        rows = []
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
+                sm_mhz, max_mhz = float(parts[2]), float(parts[3])
             except ValueError:
                 continue
-            for nm, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
+            try:
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f")
+            except ValueError:
+                ts = None
+            rows.append((ts, sm_mhz, max_mhz, parts[6:10]))
         os.unlink(self.path)
-        if not sm:
+        t0 = self.t0 or self.t1
+        if any(r[0] is None for r in rows):  # unreadable timestamps: every sample counts
+            inside = rows
+        else:
+            inside = [r for r in rows if t0 <= r[0] <= self.t1]
+        if not inside and rows and rows[0][0] is not None:  # region shorter than the period: the neighbours
+            before = [r for r in rows if r[0] < t0]
+            after = [r for r in rows if r[0] > self.t1]
+            inside = before[-1:] + after[:1]
+        if not inside:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = {nm for r in inside for nm, v in zip(names, r[3]) if v.lower().startswith("active")}
+        sm = [r[1] for r in inside]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(r[2] for r in inside)),
+                "reasons": sorted(reasons), "samples": len(sm),
+                "region_s": round((self.t1 - t0).total_seconds(), 3)}
 
 
 # ----------------------------------------------------------------- CPU side
@@ -673,6 +705,8 @@ def run_ours(args) -> None:
         clocks = ClockSampler(gpu_id) if timed else None
         barrier()
         torch.cuda.synchronize()
+        if clocks:
+            clocks.begin()
         step_ms, layer_ms = [], np.zeros(len(layers))
         for _ in range(args.steps):
             flush.zero_()
@@ -724,6 +758,8 @@ def run_ours(args) -> None:
         clocks = ClockSampler(gpu_id) if timed else None
         barrier()
         torch.cuda.synchronize()
+        if clocks:
+            clocks.begin()
         step_ms, kern_ms = [], []
         for _ in range(args.steps):
             flush.zero_()
