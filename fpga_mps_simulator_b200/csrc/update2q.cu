@@ -138,19 +138,24 @@ struct Rot {
 
 // Jacobi thresholds.  A rotation is applied when |g|^2 > tol2 a b.  The sweeps
 // end after a sweep in which no rotation had |g|^2 > stop2 a b, stop2 = 2 tol
-// (relative |g| <= 1.4e-7 at tol = 1e-14).  In its last sweeps one-sided
-// Jacobi converges quadratically, so a further sweep would find only
-// rotations far below that bound: their effect on the singular values is of
-// second order and on the columns' orthogonality below 1e-13, and the sweep
-// that would merely confirm convergence -- a full sweep of inner products
-// rotating next to nothing -- is skipped.  Checked first by emulation on the
-// theta of Haar brickwork, a CZ ansatz and XXZ Trotter evolution (singular
-// values equal to the confirmed run's, orthogonality within 1e-14); on
-// 100-site chi = 64 Haar brickwork the mean sweeps per pair fall from 8.75
-// to 7.98 (FP64).
+// (relative |g| <= 1.4e-7 at tol = 1e-14), and no rotation above tol paired
+// two columns whose squared norms lie within kStopGap of each other.  In its
+// last sweeps one-sided Jacobi converges quadratically, with a constant that
+// grows as the gap between the two singular values shrinks: a further sweep
+// would leave off-diagonals of order (relative |g|)^2 / gap, here below
+// 2e-12, while between (nearly) equal singular values convergence is linear
+// and the plain rule -- nothing above tol -- still applies.  The sweep that
+// would merely confirm convergence, a full sweep of inner products rotating
+// next to nothing, is skipped.  Checked by emulation of this kernel's rotation
+// order on the theta of Haar brickwork, a CZ ansatz, XXZ Trotter evolution
+// and spectra with exact degeneracies (column orthogonality within 1e-14, as
+// with the plain rule; without the gap condition a fully degenerate spectrum
+// stopped at 7e-9); on 100-site chi = 64 Haar brickwork the mean sweeps per
+// pair fall from 8.75 to about 8 (FP64).
 struct JTol {
     double tol2, stop2;
 };
+constexpr double kStopGap = 1e-2;
 __host__ __device__ inline double jacobi_stop2(double tol) { return 2.0 * tol > tol * tol ? 2.0 * tol : tol * tol; }
 
 __device__ __forceinline__ Rot jacobi_rotation(double a, double b, double gr, double gi, double tol2) {
@@ -323,8 +328,10 @@ __device__ __forceinline__ int rotate4(double2 (&x0)[RPL], double2 (&y0)[RPL], d
     const double a = j == 0 ? a0 : (j == 1 ? a1 : (j == 2 ? a2 : a3));
     const double b = j == 0 ? b0 : (j == 1 ? b1 : (j == 2 ? b2 : b3));
     const Rot mine = jacobi_rotation(a, b, kr, ki, jt.tol2);
-    // counted once per rotation (by its group's first lane) when still large
-    const int big = ((lane & 7) == 0) && (fma(kr, kr, ki * ki) > jt.stop2 * (a * b));
+    // counted once per rotation (by its group's first lane) when it keeps the sweeps going
+    const double g2 = fma(kr, kr, ki * ki);
+    const double thr = fabs(b - a) < kStopGap * (a + b) ? jt.tol2 : jt.stop2;
+    const int big = ((lane & 7) == 0) && (g2 > thr * (a * b));
     if constexpr (RPL >= 4) {
         // 128 rows: register-bound, so two rotations per vote (8 % faster than
         // one, while four at a time spills into a 40 % slowdown)

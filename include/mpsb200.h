@@ -140,7 +140,8 @@ MPSB_API size_t mpsb_update2q_workspace_bytes(int npairs, int chi_cap);
  *   chains, pairs, gates: device.  chi_cap: largest bond of any chain touched.
  *   tol: Jacobi off-diagonal tolerance (<= 0 picks the form's default): a column
  *        pair rotates when |x^H y|^2 > tol^2 |x|^2 |y|^2; the sweeps end after a
- *        sweep in which no pair had |x^H y|^2 > 2 tol |x|^2 |y|^2.
+ *        sweep in which no pair had |x^H y|^2 > 2 tol |x|^2 |y|^2 and no pair
+ *        whose squared norms lie within 1 % of each other rotated at all.
  *   max_sweeps: Jacobi sweep bound (<= 0 picks 40).
  *   spectra (nullable): npairs_out x 128 doubles, full descending spectrum.
  *   kept, trunc (nullable): kept count and discarded weight dropped/total.
