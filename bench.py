@@ -47,7 +47,7 @@ WORKLOAD = (f"MPS two-site updates: n={N_SITES} open chain, depth-{DEPTH} Haar b
 # DRAM bytes (read + write) of one dataflow launch (the whole 990-update step,
 # mixed form), from one ncu capture of this workload: 1.15 MB read + 3.36 MB
 # written (sites and theta copies stay in L2).
-TRAFFIC_PER_LAUNCH = 5.25e6
+TRAFFIC_PER_LAUNCH = 5.30e6
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one dataflow launch of this "
                   "workload (990 updates); algorithmic site bytes per step in hbm_site_bytes_per_step")
 
