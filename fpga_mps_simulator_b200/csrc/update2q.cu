@@ -158,11 +158,14 @@ struct JTol {
 constexpr double kStopGap = 1e-2;
 __host__ __device__ inline double jacobi_stop2(double tol) { return 2.0 * tol > tol * tol ? 2.0 * tol : tol * tol; }
 
-__device__ __forceinline__ Rot jacobi_rotation(double a, double b, double gr, double gi, double tol2) {
+__device__ __forceinline__ Rot jacobi_rotation(double a, double b, double gr, double gi, JTol jt, int &keep) {
     Rot r;
+    const double tol2 = jt.tol2;
     const double g2 = fma(gr, gr, gi * gi);
-    const bool go = (g2 > tol2 * (a * b)) && (g2 > 0.0);
+    const double ab = a * b;
+    const bool go = (g2 > tol2 * ab) && (g2 > 0.0);
     const double d = b - a;
+    keep = g2 > (fabs(d) < kStopGap * (a + b) ? tol2 : jt.stop2) * ab;
     const double w = rsqrt(fma(4.0, g2, d * d));
     const double h = fma(0.5 * fabs(d), w, 0.5);
     const double q = rsqrt(h);
@@ -327,11 +330,10 @@ __device__ __forceinline__ int rotate4(double2 (&x0)[RPL], double2 (&y0)[RPL], d
     const int j = lane >> 3;
     const double a = j == 0 ? a0 : (j == 1 ? a1 : (j == 2 ? a2 : a3));
     const double b = j == 0 ? b0 : (j == 1 ? b1 : (j == 2 ? b2 : b3));
-    const Rot mine = jacobi_rotation(a, b, kr, ki, jt.tol2);
+    int keep;
+    const Rot mine = jacobi_rotation(a, b, kr, ki, jt, keep);
     // counted once per rotation (by its group's first lane) when it keeps the sweeps going
-    const double g2 = fma(kr, kr, ki * ki);
-    const double thr = fabs(b - a) < kStopGap * (a + b) ? jt.tol2 : jt.stop2;
-    const int big = ((lane & 7) == 0) && (g2 > thr * (a * b));
+    const int big = ((lane & 7) == 0) && keep;
     if constexpr (RPL >= 4) {
         // 128 rows: register-bound, so two rotations per vote (8 % faster than
         // one, while four at a time spills into a 40 % slowdown)
