@@ -241,20 +241,21 @@ def gradient_leg(dev, steps: int, warmup: int, rank: int, max_over_ranks, cpu_wo
         torch.cuda.reset_peak_memory_stats(dev)
         base_mem = torch.cuda.memory_allocated(dev)
         model.engine.launches = 0
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(steps):
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        evs[0].record()
+        for k in range(steps):
             E, g = model.energy_and_grad(angles)
-        e1.record()
+            evs[k + 1].record()
         torch.cuda.synchronize()
-        sec = max_over_ranks(e0.elapsed_time(e1) * 1e-3) / steps
+        sec = max_over_ranks(evs[0].elapsed_time(evs[-1]) * 1e-3) / steps
+        step_s = [round(evs[k].elapsed_time(evs[k + 1]) * 1e-3, 5) for k in range(steps)]
         key = prec if ckpt == "auto" else f"{prec}_checkpointed"
         grads[key] = (E.clone(), g.clone())
         if ckpt == "auto":
             finals[prec] = model.batch
         if flops is None:
             flops = hea_grad_flops(model, angles)
-        out[key] = {"s_per_grad_step": round(sec, 5), "grad_steps_per_s": round(1.0 / sec, 4),
+        out[key] = {"s_per_grad_step": round(sec, 5), "step_s": step_s, "grad_steps_per_s": round(1.0 / sec, 4),
                     "param_vectors_per_s": round(GRAD_VEC / sec, 3),
                     "recompute": bool(model.engine.checkpointed),
                     "launches_per_step": model.engine.launches // steps,
@@ -933,7 +934,7 @@ def run_ours(args) -> None:
         from oracle.cpu_baseline import usable_cores
         cw = usable_cores() if (rank == 0 and world == 1 and not args.no_cpu) else 0
         torch.cuda.empty_cache()  # the 7.6 GB of tapes below should not fight the earlier legs' cached blocks
-        gradient = gradient_leg(dev, 5, 3, rank, max_over_ranks, cpu_workers=cw)
+        gradient = gradient_leg(dev, 5, 5, rank, max_over_ranks, cpu_workers=cw)
         for key in ("fp64", "mixed", "mixed_all", "fp64_checkpointed"):  # fraction of the same FP64 roofline
             gradient[key]["roofline_frac"] = round(gradient[key]["achieved_tflops"] / fp64_peak_tflops, 4)
 
